@@ -1,0 +1,468 @@
+// C ABI: device graphs and search workers (include/everest_b200.h).
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "evx_internal.cuh"
+
+namespace evx {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();  // clear a sticky launch error where possible
+  return fail(e == cudaErrorMemoryAllocation ? EVX_ERR_NOMEM : EVX_ERR_CUDA, m);
+}
+
+int graph_t_range(DeviceGraph &g, int *scratch_d, cudaStream_t s);
+
+// Decode a relabeled motif into the per-level plan (HostMotifData rules,
+// src/core/cpu/data.cc:416-446).
+static int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
+  if (k < 2 || k > EVX_MAX_MOTIF_EDGES)
+    return fail(EVX_ERR_INVALID, "motif must have 2.." + std::to_string(EVX_MAX_MOTIF_EDGES) + " edges");
+  if (mu[0] != 0 || mv[0] != 1)
+    return fail(EVX_ERR_INVALID, "motif edge 0 must be (0, 1) after relabeling");
+  std::memset(plan, 0, sizeof(*plan));
+  plan->k = k;
+  int nm = 2;
+  for (int j = 1; j < k; j++) {
+    const int a = mu[j], b = mv[j];
+    if (a < 0 || b < 0 || a == b)
+      return fail(EVX_ERR_INVALID, "motif edge " + std::to_string(j) + " is a self-loop or negative");
+    const bool an = a >= nm, bn = b >= nm;
+    if (an && bn)
+      return fail(EVX_ERR_INVALID, "motif edge " + std::to_string(j) + " touches no mapped node");
+    int kind;
+    if (an) {
+      if (a != nm) return fail(EVX_ERR_INVALID, "motif nodes are not numbered by first appearance");
+      kind = 0;
+    } else if (bn) {
+      if (b != nm) return fail(EVX_ERR_INVALID, "motif nodes are not numbered by first appearance");
+      kind = 1;
+    } else {
+      kind = 2;
+    }
+    plan->info[j - 1] = kind | (a << 4) | (b << 8) | (nm << 12);
+    if (an || bn) nm++;
+    if (nm > EVX_MAX_MOTIF_NODES)
+      return fail(EVX_ERR_INVALID, "motif has too many nodes");
+  }
+  plan->n = nm;
+  return EVX_OK;
+}
+
+}  // namespace evx
+
+using namespace evx;
+
+struct evx_graph {
+  DeviceGraph g;
+};
+
+struct evx_worker {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 148;
+  // small device state: [0] u64 count, [2] int cursor, [3] int stop, [4..5] t range scratch
+  unsigned long long *state_d = nullptr;
+  unsigned long long *count_h = nullptr;  // pinned
+  int *rows_d = nullptr;
+  int64_t rows_cap = 0;  // allocated rows
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // bound job
+  bool has_job = false;
+  bool launched = false;
+  GraphView view{};
+  MotifPlan plan{};
+  SearchArgs args{};
+  int64_t enum_cap = 0;
+  uint64_t last_count = 0;
+  // tuning
+  int block = 256, blocks_per_sm = 0, roots_per_fetch = 32, steal_interval = 16, min_split = 2;
+  int last_launches = 0;
+  float last_ms = 0.f;
+};
+
+extern "C" {
+
+const char *evx_last_error(void) { return g_last_error.c_str(); }
+
+int evx_device_count(int *count) {
+  if (!count) return fail(EVX_ERR_INVALID, "null count");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  *count = n;
+  return EVX_OK;
+}
+
+static int alloc_graph(int device, int64_t E, int64_t V, evx_graph **out, cudaStream_t s) {
+  if (!out) return fail(EVX_ERR_INVALID, "null output pointer");
+  if (E < 0 || V < 0) return fail(EVX_ERR_INVALID, "negative sizes");
+  if (E >= INT_MAX / 2 || V >= INT_MAX - 1)
+    return fail(EVX_ERR_OVERFLOW, "graph too large for int32 edge / vertex ids");
+  int ndev = 0;
+  evx_device_count(&ndev);
+  if (ndev == 0) return fail(EVX_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(EVX_ERR_INVALID, "bad device index");
+  EVX_CUDA(cudaSetDevice(device));
+  evx_graph *h = new (std::nothrow) evx_graph();
+  if (!h) return fail(EVX_ERR_NOMEM, "host allocation failed");
+  DeviceGraph &g = h->g;
+  g.device = device;
+  g.num_edges = E;
+  g.num_vertices = V;
+  const size_t e1 = (size_t)(E > 0 ? E : 1);
+  size_t bytes = 0;
+  cudaError_t err = cudaSuccess;
+  auto A = [&](void **p, size_t n) {
+    if (err == cudaSuccess) { err = cudaMalloc(p, n); bytes += n; }
+  };
+  A((void **)&g.edges, sizeof(int4) * e1);
+  A((void **)&g.rootpos, sizeof(int2) * e1);
+  A((void **)&g.out_rec, sizeof(int4) * e1);
+  A((void **)&g.in_rec, sizeof(int4) * e1);
+  A((void **)&g.out_off, sizeof(int) * (size_t)(V + 1));
+  A((void **)&g.in_off, sizeof(int) * (size_t)(V + 1));
+  g.bytes = (int64_t)bytes;
+  if (err != cudaSuccess) {
+    cudaFree(g.edges); cudaFree(g.rootpos); cudaFree(g.out_rec); cudaFree(g.in_rec);
+    cudaFree(g.out_off); cudaFree(g.in_off);
+    delete h;
+    return cuda_fail(err, "cudaMalloc(device graph)");
+  }
+  (void)s;
+  *out = h;
+  return EVX_OK;
+}
+
+static int finish_graph(evx_graph *h, cudaStream_t s) {
+  int *scratch = nullptr;
+  EVX_CUDA(cudaMalloc(&scratch, 2 * sizeof(int)));
+  int rc = graph_t_range(h->g, scratch, s);
+  cudaFree(scratch);
+  return rc;
+}
+
+int evx_graph_from_device(int device, int64_t num_edges, int64_t num_vertices, const int *eg_d,
+                          const int *out_v_d, const int *in_v_d, const int *out_r_d,
+                          const int *in_r_d, const int *euid_d, void *stream, evx_graph **out) {
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = alloc_graph(device, num_edges, num_vertices, out, s);
+  if (rc) return rc;
+  rc = pack_graph((*out)->g, eg_d, out_v_d, in_v_d, out_r_d, in_r_d, euid_d, s);
+  if (!rc) rc = finish_graph(*out, s);
+  if (rc) { evx_graph_free(*out); *out = nullptr; }
+  return rc;
+}
+
+int evx_graph_upload(int device, int64_t num_edges, int64_t num_vertices, const int *eg,
+                     const int *out_v, const int *in_v, const int *out_r, const int *in_r,
+                     const int *euid, void *stream, evx_graph **out) {
+  if (!out || (num_edges > 0 && (!eg || !out_v || !in_v)) || !out_r || !in_r)
+    return fail(EVX_ERR_INVALID, "null graph array");
+  cudaStream_t s = (cudaStream_t)stream;
+  {
+    // The packing kernels index with these arrays: reject anything that
+    // would send them out of bounds.
+    const int64_t E = num_edges, V = num_vertices;
+    if (E < 0 || V < 0) return fail(EVX_ERR_INVALID, "negative sizes");
+    if (out_r[0] != 0 || in_r[0] != 0 || out_r[V] != E || in_r[V] != E)
+      return fail(EVX_ERR_INVALID, "CSR offsets must start at 0 and end at num_edges");
+    for (int64_t x = 0; x < V; x++)
+      if (out_r[x + 1] < out_r[x] || in_r[x + 1] < in_r[x])
+        return fail(EVX_ERR_INVALID, "CSR offsets are not monotone");
+    for (int64_t i = 0; i < E; i++) {
+      if ((unsigned)out_v[i] >= (uint64_t)E || (unsigned)in_v[i] >= (uint64_t)E)
+        return fail(EVX_ERR_INVALID, "edge id out of range in out/in lists");
+      if ((unsigned)eg[3 * i] >= (uint64_t)V || (unsigned)eg[3 * i + 1] >= (uint64_t)V)
+        return fail(EVX_ERR_INVALID, "vertex id out of range in Eg");
+      if (i && eg[3 * i + 2] < eg[3 * i - 1])
+        return fail(EVX_ERR_INVALID, "edges are not sorted by timestamp");
+    }
+  }
+  int rc = alloc_graph(device, num_edges, num_vertices, out, s);
+  if (rc) return rc;
+  const size_t E = (size_t)(num_edges > 0 ? num_edges : 1), V1 = (size_t)num_vertices + 1;
+  // staging in host-format layout (freed after packing)
+  int *buf = nullptr;
+  const size_t n_ints = 3 * E + E + E + V1 + V1 + E;
+  cudaError_t err = cudaMalloc(&buf, n_ints * sizeof(int));
+  if (err != cudaSuccess) {
+    evx_graph_free(*out);
+    *out = nullptr;
+    return cuda_fail(err, "cudaMalloc(upload staging)");
+  }
+  int *eg_d = buf, *ov_d = eg_d + 3 * E, *iv_d = ov_d + E, *or_d = iv_d + E, *ir_d = or_d + V1,
+      *eu_d = ir_d + V1;
+  const size_t ne = (size_t)num_edges;
+  rc = EVX_OK;
+  auto C = [&](void *d, const void *h, size_t n) {
+    if (rc == EVX_OK && n) {
+      cudaError_t e = cudaMemcpyAsync(d, h, n, cudaMemcpyHostToDevice, s);
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(upload)");
+    }
+  };
+  C(eg_d, eg, sizeof(int) * 3 * ne);
+  C(ov_d, out_v, sizeof(int) * ne);
+  C(iv_d, in_v, sizeof(int) * ne);
+  C(or_d, out_r, sizeof(int) * V1);
+  C(ir_d, in_r, sizeof(int) * V1);
+  if (euid) C(eu_d, euid, sizeof(int) * ne);
+  if (!rc) rc = pack_graph((*out)->g, eg_d, ov_d, iv_d, or_d, ir_d, euid ? eu_d : nullptr, s);
+  if (!rc) rc = finish_graph(*out, s);
+  cudaStreamSynchronize(s);
+  cudaFree(buf);
+  if (rc) { evx_graph_free(*out); *out = nullptr; }
+  return rc;
+}
+
+int evx_graph_free(evx_graph *h) {
+  if (!h) return EVX_OK;
+  DeviceGraph &g = h->g;
+  cudaSetDevice(g.device);
+  cudaFree(g.edges); cudaFree(g.rootpos); cudaFree(g.out_rec); cudaFree(g.in_rec);
+  cudaFree(g.out_off); cudaFree(g.in_off);
+  delete h;
+  return EVX_OK;
+}
+
+int evx_graph_info(const evx_graph *h, int64_t *num_edges, int64_t *num_vertices, int *device,
+                   int64_t *device_bytes) {
+  if (!h) return fail(EVX_ERR_INVALID, "null graph");
+  if (num_edges) *num_edges = h->g.num_edges;
+  if (num_vertices) *num_vertices = h->g.num_vertices;
+  if (device) *device = h->g.device;
+  if (device_bytes) *device_bytes = h->g.bytes;
+  return EVX_OK;
+}
+
+int evx_worker_create(int device, void *stream, evx_worker **out) {
+  if (!out) return fail(EVX_ERR_INVALID, "null output pointer");
+  int ndev = 0;
+  evx_device_count(&ndev);
+  if (ndev == 0) return fail(EVX_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(EVX_ERR_INVALID, "bad device index");
+  EVX_CUDA(cudaSetDevice(device));
+  evx_worker *w = new (std::nothrow) evx_worker();
+  if (!w) return fail(EVX_ERR_NOMEM, "host allocation failed");
+  w->device = device;
+  cudaDeviceGetAttribute(&w->num_sms, cudaDevAttrMultiProcessorCount, device);
+  cudaError_t e = cudaSuccess;
+  if (stream) {
+    w->stream = (cudaStream_t)stream;
+  } else {
+    e = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
+    w->own_stream = true;
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&w->state_d, 64);
+  if (e == cudaSuccess) e = cudaMemset(w->state_d, 0, 64);
+  if (e == cudaSuccess) e = cudaMallocHost(&w->count_h, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaEventCreate(&w->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&w->ev1);
+  if (e != cudaSuccess) {
+    evx_worker_destroy(w);
+    return cuda_fail(e, "worker setup");
+  }
+  *out = w;
+  return EVX_OK;
+}
+
+int evx_worker_destroy(evx_worker *w) {
+  if (!w) return EVX_OK;
+  cudaSetDevice(w->device);
+  if (w->stream) cudaStreamSynchronize(w->stream);
+  cudaFree(w->state_d);
+  cudaFree(w->rows_d);
+  if (w->count_h) cudaFreeHost(w->count_h);
+  if (w->ev0) cudaEventDestroy(w->ev0);
+  if (w->ev1) cudaEventDestroy(w->ev1);
+  if (w->own_stream && w->stream) cudaStreamDestroy(w->stream);
+  delete w;
+  return EVX_OK;
+}
+
+int evx_worker_stream(evx_worker *w, void **stream) {
+  if (!w || !stream) return fail(EVX_ERR_INVALID, "null argument");
+  *stream = (void *)w->stream;
+  return EVX_OK;
+}
+
+int evx_worker_set_tuning(evx_worker *w, int block, int blocks_per_sm, int roots_per_fetch,
+                          int steal_interval, int min_split) {
+  if (!w) return fail(EVX_ERR_INVALID, "null worker");
+  if (block < 32 || block > 256 || block % 32)
+    return fail(EVX_ERR_INVALID, "block must be a multiple of 32 in [32, 256]");
+  if (blocks_per_sm < 0 || roots_per_fetch < 1 || roots_per_fetch > 4096 || steal_interval < 0 ||
+      min_split < 2)
+    return fail(EVX_ERR_INVALID, "bad tuning value");
+  if (steal_interval & (steal_interval - 1))
+    return fail(EVX_ERR_INVALID, "steal_interval must be 0 or a power of two");
+  w->block = block;
+  w->blocks_per_sm = blocks_per_sm;
+  w->roots_per_fetch = roots_per_fetch;
+  w->steal_interval = steal_interval;
+  w->min_split = min_split;
+  return EVX_OK;
+}
+
+int evx_worker_take(evx_worker *w, const evx_graph *gh, int k, const int *mu, const int *mv,
+                    int delta, int64_t beg, int64_t end, int64_t enum_cap, unsigned flags) {
+  if (!w || !gh || !mu || !mv) return fail(EVX_ERR_INVALID, "null argument");
+  if (gh->g.device != w->device) return fail(EVX_ERR_INVALID, "graph and worker on different devices");
+  MotifPlan plan;
+  int rc = build_plan(k, mu, mv, &plan);
+  if (rc) return rc;
+  const DeviceGraph &g = gh->g;
+  if (delta < 0) return fail(EVX_ERR_INVALID, "delta must be non-negative");
+  if ((int64_t)g.max_t + (int64_t)delta > (int64_t)INT_MAX)
+    return fail(EVX_ERR_OVERFLOW, "t + delta overflows int32 (max t " + std::to_string(g.max_t) +
+                                      ", delta " + std::to_string(delta) + ")");
+  const int64_t E = g.num_edges;
+  if (end < 0) end = E - k + 1;
+  if (end > E) end = E;
+  if (beg < 0) beg = 0;
+  if (end < beg) end = beg;
+  EVX_CUDA(cudaSetDevice(w->device));
+  if (enum_cap > 0) {
+    if (enum_cap > (int64_t)INT_MAX) return fail(EVX_ERR_INVALID, "enumeration cap too large");
+    const int64_t need = enum_cap * (int64_t)k;
+    if (need > w->rows_cap) {
+      size_t fr = 0, tot = 0;
+      EVX_CUDA(cudaMemGetInfo(&fr, &tot));
+      const size_t bytes = (size_t)need * sizeof(int);
+      const size_t reserve = (size_t)256 << 20;  // keep headroom for other work
+      if (bytes + reserve > fr)
+        return fail(EVX_ERR_NOMEM, "enumeration buffer of " + std::to_string(bytes) +
+                                       " bytes not admitted (free " + std::to_string(fr) + ")");
+      if (w->rows_d) { cudaFree(w->rows_d); w->rows_d = nullptr; w->rows_cap = 0; }
+      EVX_CUDA(cudaMalloc(&w->rows_d, bytes));
+      w->rows_cap = need;
+    }
+  }
+  w->view = g.view();
+  w->plan = plan;
+  SearchArgs &a = w->args;
+  std::memset(&a, 0, sizeof(a));
+  a.root_beg = (int)beg;
+  a.root_end = (int)end;
+  a.delta = delta;
+  a.strict_ts = (flags & EVX_FLAG_STRICT_TS) ? 1 : 0;
+  a.roots_per_fetch = w->roots_per_fetch;
+  a.steal_interval = (flags & EVX_FLAG_NO_STEAL) ? 0 : w->steal_interval;
+  a.min_split = w->min_split;
+  a.enumerate = enum_cap > 0 ? 1 : 0;
+  a.exact_total = (flags & EVX_FLAG_EXACT_TOTAL) ? 1 : 0;
+  a.cap = enum_cap;
+  a.rows = w->rows_d;
+  a.count = w->state_d;
+  a.cursor = reinterpret_cast<int *>(w->state_d + 1);
+  a.stop = reinterpret_cast<int *>(w->state_d + 1) + 1;
+  w->enum_cap = enum_cap;
+  w->has_job = true;
+  w->launched = false;
+  return EVX_OK;
+}
+
+namespace evx {
+__global__ void reset_state_kernel(unsigned long long *count, int *cursor, int *stop, int beg) {
+  *count = 0ull;
+  *cursor = beg;
+  *stop = 0;
+}
+}  // namespace evx
+
+int evx_worker_launch(evx_worker *w) {
+  if (!w) return fail(EVX_ERR_INVALID, "null worker");
+  if (!w->has_job) return fail(EVX_ERR_STATE, "run before take");
+  EVX_CUDA(cudaSetDevice(w->device));
+  SearchArgs &a = w->args;
+  int bps = w->blocks_per_sm;
+  if (bps <= 0) {
+    int rc = search_occupancy(w->plan.k, a.enumerate != 0, w->block, &bps);
+    if (rc) return rc;
+    if (bps <= 0) bps = 1;
+  }
+  const int grid = bps * w->num_sms;
+  const int64_t warps = (int64_t)grid * (w->block / 32);
+  if ((int64_t)a.root_end + warps * (int64_t)a.roots_per_fetch >= (int64_t)INT_MAX)
+    return fail(EVX_ERR_OVERFLOW, "root cursor would overflow int32");
+  reset_state_kernel<<<1, 1, 0, w->stream>>>(a.count, a.cursor, a.stop, a.root_beg);
+  EVX_CUDA(cudaGetLastError());
+  EVX_CUDA(cudaEventRecord(w->ev0, w->stream));
+  int launches = 1;
+  if (a.root_end > a.root_beg) {
+    int rc = launch_search(w->view, w->plan, a, grid, w->block, w->stream);
+    if (rc) return rc;
+    EVX_CUDA(cudaGetLastError());
+    launches++;
+  }
+  EVX_CUDA(cudaEventRecord(w->ev1, w->stream));
+  EVX_CUDA(cudaMemcpyAsync(w->count_h, a.count, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           w->stream));
+  w->last_launches = launches;
+  w->launched = true;
+  return EVX_OK;
+}
+
+int evx_worker_result(evx_worker *w, uint64_t *count) {
+  if (!w || !count) return fail(EVX_ERR_INVALID, "null argument");
+  if (!w->launched) return fail(EVX_ERR_STATE, "result before launch");
+  EVX_CUDA(cudaSetDevice(w->device));
+  EVX_CUDA(cudaStreamSynchronize(w->stream));
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, w->ev0, w->ev1) == cudaSuccess) w->last_ms = ms;
+  w->last_count = *w->count_h;
+  *count = w->last_count;
+  w->launched = false;
+  return EVX_OK;
+}
+
+int evx_worker_run(evx_worker *w, uint64_t *count) {
+  int rc = evx_worker_launch(w);
+  if (rc) return rc;
+  return evx_worker_result(w, count);
+}
+
+int evx_worker_enum_rows(evx_worker *w, int64_t n, int *rows, int64_t *rows_written) {
+  if (!w || (n > 0 && !rows)) return fail(EVX_ERR_INVALID, "null argument");
+  if (!w->has_job || w->enum_cap <= 0) return fail(EVX_ERR_STATE, "no enumeration job");
+  int64_t f = n;
+  if ((int64_t)w->last_count < f) f = (int64_t)w->last_count;
+  if (w->enum_cap < f) f = w->enum_cap;
+  if (f < 0) f = 0;
+  if (f > 0) {
+    EVX_CUDA(cudaSetDevice(w->device));
+    EVX_CUDA(cudaMemcpyAsync(rows, w->rows_d, sizeof(int) * (size_t)f * w->plan.k,
+                             cudaMemcpyDeviceToHost, w->stream));
+    EVX_CUDA(cudaStreamSynchronize(w->stream));
+  }
+  if (rows_written) *rows_written = f;
+  return EVX_OK;
+}
+
+int evx_worker_last_stats(evx_worker *w, int *kernel_launches, float *device_ms) {
+  if (!w) return fail(EVX_ERR_INVALID, "null worker");
+  if (kernel_launches) *kernel_launches = w->last_launches;
+  if (device_ms) *device_ms = w->last_ms;
+  return EVX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,107 @@
+// Device graph: upload of the host graph arrays and on-device packing into
+// the 16-byte record layout the search kernels read.
+//
+// Host-format inputs are the reference's HostGraphData arrays
+// (include/data.h:174-186): Eg (AoS {u,v,t}), outEdgesV / inEdgesV (edge ids
+// grouped by endpoint, ascending), outEdgesR / inEdgesR (CSR offsets) and
+// Euid.  The upload moves exactly those bytes (24 E + 8 (V+1), as
+// calcTotalBytes, src/core/gpu/data.cu:22-24) and expands them on the device:
+//   edges[e]   = {u, v, t, euid}
+//   rootpos[e] = {position of e in out_rec, position of e in in_rec}
+//   out_rec[p] = {eid, v, t, position of eid in in_rec}
+//   in_rec[p]  = {eid, u, t, position of eid in out_rec}
+#include <climits>
+
+#include "evx_internal.cuh"
+
+namespace evx {
+namespace {
+
+__global__ void pack_edges_kernel(const int *__restrict__ eg, const int *__restrict__ euid,
+                                  int4 *__restrict__ edges, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    edges[i] = make_int4(eg[3 * i], eg[3 * i + 1], eg[3 * i + 2], euid ? euid[i] : i);
+  }
+}
+
+__global__ void scatter_pos_kernel(const int *__restrict__ out_v, const int *__restrict__ in_v,
+                                   int2 *__restrict__ rootpos, int n) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    rootpos[out_v[p]].x = p;
+    rootpos[in_v[p]].y = p;
+  }
+}
+
+__global__ void pack_rec_kernel(const int *__restrict__ out_v, const int *__restrict__ in_v,
+                                const int4 *__restrict__ edges, const int2 *__restrict__ rootpos,
+                                int4 *__restrict__ out_rec, int4 *__restrict__ in_rec, int n) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int eo = out_v[p];
+    const int4 a = edges[eo];
+    out_rec[p] = make_int4(eo, a.y, a.z, rootpos[eo].y);
+    const int ei = in_v[p];
+    const int4 b = edges[ei];
+    in_rec[p] = make_int4(ei, b.x, b.z, rootpos[ei].x);
+  }
+}
+
+// min / max timestamp (for the t + delta overflow check)
+__global__ void t_range_kernel(const int4 *__restrict__ edges, int n, int *out) {
+  int lo = INT_MAX, hi = INT_MIN;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int t = edges[i].z;
+    lo = min(lo, t);
+    hi = max(hi, t);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_down_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_down_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(out, lo);
+    atomicMax(out + 1, hi);
+  }
+}
+
+__global__ void t_range_init_kernel(int *out) {
+  out[0] = INT_MAX;
+  out[1] = INT_MIN;
+}
+
+}  // namespace
+
+int pack_graph(DeviceGraph &g, const int *eg_d, const int *out_v_d, const int *in_v_d,
+               const int *out_r_d, const int *in_r_d, const int *euid_d, cudaStream_t s) {
+  const int64_t E = g.num_edges, V = g.num_vertices;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
+  const int grid = sms * 8, block = 256;
+  EVX_CUDA(cudaMemcpyAsync(g.out_off, out_r_d, sizeof(int) * (V + 1), cudaMemcpyDeviceToDevice, s));
+  EVX_CUDA(cudaMemcpyAsync(g.in_off, in_r_d, sizeof(int) * (V + 1), cudaMemcpyDeviceToDevice, s));
+  if (E > 0) {
+    pack_edges_kernel<<<grid, block, 0, s>>>(eg_d, euid_d, g.edges, (int)E);
+    scatter_pos_kernel<<<grid, block, 0, s>>>(out_v_d, in_v_d, g.rootpos, (int)E);
+    pack_rec_kernel<<<grid, block, 0, s>>>(out_v_d, in_v_d, g.edges, g.rootpos, g.out_rec,
+                                           g.in_rec, (int)E);
+  }
+  EVX_CUDA(cudaGetLastError());
+  return EVX_OK;
+}
+
+int graph_t_range(DeviceGraph &g, int *scratch_d, cudaStream_t s) {
+  int h[2] = {0, 0};
+  t_range_init_kernel<<<1, 1, 0, s>>>(scratch_d);
+  if (g.num_edges > 0) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
+    t_range_kernel<<<sms * 4, 256, 0, s>>>(g.edges, (int)g.num_edges, scratch_d);
+  }
+  EVX_CUDA(cudaGetLastError());
+  EVX_CUDA(cudaMemcpyAsync(h, scratch_d, sizeof(h), cudaMemcpyDeviceToHost, s));
+  EVX_CUDA(cudaStreamSynchronize(s));
+  g.min_t = g.num_edges ? h[0] : 0;
+  g.max_t = g.num_edges ? h[1] : 0;
+  return EVX_OK;
+}
+
+}  // namespace evx

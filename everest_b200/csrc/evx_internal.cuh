@@ -1,0 +1,106 @@
+// Internal types shared by the device graph, search kernels and C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/everest_b200.h"
+
+namespace evx {
+
+// Device layout of one graph (all int32; E < 2^31, V < 2^31).
+//   edges[e]   = {u, v, t, euid}                     root fetch + enumeration
+//   rootpos[e] = {pos of e in out_rec, pos of e in in_rec}   (absolute)
+//   out_rec[p] = {eid, v, t, pos of eid in in_rec}    grouped by u, ascending eid
+//   in_rec[p]  = {eid, u, t, pos of eid in out_rec}   grouped by v, ascending eid
+//   out_off / in_off: CSR offsets [V+1] into out_rec / in_rec.
+struct GraphView {
+  const int4 *edges;
+  const int2 *rootpos;
+  const int4 *out_rec;
+  const int4 *in_rec;
+  const int *out_off;
+  const int *in_off;
+  int num_edges;
+  int num_vertices;
+};
+
+// Per-level search plan.  Level l (0-based) matches motif edge j = l + 1.
+//   kind 0: new source -> scan in-list of image(b)
+//   kind 1: new target -> scan out-list of image(a)
+//   kind 2: both mapped -> scan the shorter of in(image(b)) / out(image(a))
+// nm = nodes mapped before edge j (= index of the new node for kinds 0/1).
+// Packed as kind | a << 4 | b << 8 | nm << 12.
+struct MotifPlan {
+  int k;          // motif edges
+  int n;          // motif nodes
+  int info[EVX_MAX_MOTIF_EDGES];
+};
+
+__host__ __device__ inline int plan_kind(int w) { return w & 3; }
+__host__ __device__ inline int plan_a(int w) { return (w >> 4) & 15; }
+__host__ __device__ inline int plan_b(int w) { return (w >> 8) & 15; }
+__host__ __device__ inline int plan_nm(int w) { return (w >> 12) & 15; }
+
+// Search job arguments (one query).
+struct SearchArgs {
+  int root_beg, root_end;     // root edge ids [beg, end)
+  int delta;
+  int strict_ts;
+  int roots_per_fetch;        // roots claimed per warp refill (multiple of 1)
+  int steal_interval;         // iterations between steal checks (power of 2), 0 = off
+  int min_split;              // smallest range width worth splitting
+  int enumerate;              // 1: write rows
+  int exact_total;            // enumerate: keep counting past the cap
+  long long cap;              // enumeration rows capacity
+  int *rows;                  // [cap * k] original line ids
+  unsigned long long *count;  // [1] result / enumeration slot counter
+  int *cursor;                // [1] next unclaimed root id
+  int *stop;                  // [1] set when the enumeration cap is reached
+};
+
+// Host-side graph object.
+struct DeviceGraph {
+  int device = 0;
+  int64_t num_edges = 0, num_vertices = 0;
+  int max_t = 0, min_t = 0;
+  int4 *edges = nullptr;
+  int2 *rootpos = nullptr;
+  int4 *out_rec = nullptr;
+  int4 *in_rec = nullptr;
+  int *out_off = nullptr;
+  int *in_off = nullptr;
+  int64_t bytes = 0;
+  GraphView view() const {
+    GraphView g;
+    g.edges = edges; g.rootpos = rootpos; g.out_rec = out_rec; g.in_rec = in_rec;
+    g.out_off = out_off; g.in_off = in_off;
+    g.num_edges = (int)num_edges; g.num_vertices = (int)num_vertices;
+    return g;
+  }
+};
+
+// Error plumbing (thread-local message).
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define EVX_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t _e = (call);                             \
+    if (_e != cudaSuccess) return ::evx::cuda_fail(_e, #call); \
+  } while (0)
+
+// Launch the search for one query (defined in evx_search.cu).
+int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &args,
+                  int grid, int block, cudaStream_t stream);
+// Max resident blocks per SM for a given motif size / mode / block.
+int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm);
+
+// Build the packed device layout from the uploaded host-format arrays
+// (defined in evx_graph.cu).
+int pack_graph(DeviceGraph &g, const int *eg_d, const int *out_v_d, const int *in_v_d,
+               const int *out_r_d, const int *in_r_d, const int *euid_d, cudaStream_t s);
+
+}  // namespace evx

@@ -1,0 +1,162 @@
+/*
+ * everest_b200.h -- C ABI of the B200 temporal-motif miner.
+ *
+ * Plain pointers, sizes and int status codes; no C++ or torch types cross
+ * this boundary.  Every entry point returns EVX_OK (0) or a negative
+ * EVX_ERR_* code; evx_last_error() gives a thread-local message for the last
+ * failure.  No entry point exits the process (the reference's gpuErrchk
+ * calls exit(), include/helpers.cuh:7-15; this layer reports instead).
+ *
+ * Each entry point names the reference interface it replaces (paths are
+ * relative to the reference project root).
+ */
+#ifndef EVEREST_B200_H_
+#define EVEREST_B200_H_
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define EVX_API __attribute__((visibility("default")))
+#else
+#define EVX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EVX_OK 0
+#define EVX_ERR_INVALID (-1)   /* bad argument, bad motif, bad sizes */
+#define EVX_ERR_CUDA (-2)      /* CUDA runtime error */
+#define EVX_ERR_NOMEM (-3)     /* device or host allocation failed / not admitted */
+#define EVX_ERR_OVERFLOW (-4)  /* t + delta overflows int32, or sizes exceed int32 ids */
+#define EVX_ERR_IO (-5)        /* file missing or unreadable */
+#define EVX_ERR_STATE (-6)     /* call out of order (e.g. run before take) */
+#define EVX_ERR_TIMEOUT (-7)   /* a bounded device wait gave up */
+#define EVX_ERR_NODEVICE (-8)  /* no CUDA device */
+
+/* Largest motif the kernels are instantiated for. */
+#define EVX_MAX_MOTIF_EDGES 8
+#define EVX_MAX_MOTIF_NODES 9
+
+/* evx_worker_take flags */
+#define EVX_FLAG_STRICT_TS 1u    /* additionally require t(e_j) > t(e_{j-1}) */
+#define EVX_FLAG_EXACT_TOTAL 2u  /* enumerate: keep counting past the cap */
+#define EVX_FLAG_NO_STEAL 4u     /* disable intra-warp work stealing */
+
+typedef struct evx_graph evx_graph;   /* a graph resident on one device */
+typedef struct evx_worker evx_worker; /* per-device search worker */
+
+/* Thread-local message describing the last failure. */
+EVX_API const char *evx_last_error(void);
+
+/* Number of visible CUDA devices (0 when none). */
+EVX_API int evx_device_count(int *count);
+
+/* ------------------------------------------------------------ host data --
+ * Edge-list loading (replaces EdgeListLoader::createEdgeListCache,
+ * src/core/cpu/data.cc:175-290): parse "u v t" lines with atoi semantics,
+ * stable-sort by t.  On success *u, *v, *t, *ids hold malloc'd arrays of
+ * *num_edges ints (ids = original 0-based line index of each sorted edge);
+ * release them with evx_free. */
+EVX_API int evx_edgelist_parse(const char *path, int64_t *num_edges,
+                       int **u, int **v, int **t, int **ids);
+
+/* Graph building (replaces GraphDataLoader::createGraphData,
+ * src/core/gpu/data.cu:124-348): relabels vertices to 0..V-1, builds
+ * out/in edge-id lists grouped by endpoint and ascending in edge id, CSR
+ * offsets and the AoS {u,v,t} array.  Inputs are the sorted edge range
+ * [beg, end) of an edge list.  Outputs are malloc'd (evx_free):
+ *   eg[3*E], out_v[E], in_v[E], out_r[V+1], in_r[V+1], euid[E]. */
+EVX_API int evx_graph_build_host(const int *u, const int *v, const int *t,
+                         const int *ids, int64_t beg, int64_t end,
+                         int64_t *num_edges, int64_t *num_vertices,
+                         int **eg, int **out_v, int **in_v,
+                         int **out_r, int **in_r, int **euid);
+
+/* Motif decoding (replaces HostMotifData::HostMotifData,
+ * src/core/cpu/data.cc:411-449 with TemporalGraph::ReadGraph,
+ * src/core/cpu/Graph.cc:198-258): lines "u v t", stable-sorted by t, nodes
+ * relabeled by first appearance.  Writes k relabeled edges into mu/mv
+ * (capacity EVX_MAX_MOTIF_EDGES each) and the node count. */
+EVX_API int evx_motif_parse(const char *path, int *k, int *mu, int *mv, int *num_nodes);
+EVX_API int evx_motif_parse_text(const char *text, int *k, int *mu, int *mv, int *num_nodes);
+
+EVX_API void evx_free(void *p);
+
+/* --------------------------------------------------------- device graph --
+ * Allocation + host->device transfer of one graph (replaces
+ * GraphDataManager::alloc / moveAsync / waitMove,
+ * src/core/gpu/data.cu:380-467, and DeviceGraphData, include/data.h:239-247).
+ * Inputs are host arrays in the layout evx_graph_build_host produces; they
+ * may be pageable or pinned.  The device-side packed layout (16-byte
+ * adjacency records) is built on the device from them.  stream may be NULL
+ * (the worker-independent upload stream is used). */
+EVX_API int evx_graph_upload(int device, int64_t num_edges, int64_t num_vertices,
+                     const int *eg, const int *out_v, const int *in_v,
+                     const int *out_r, const int *in_r, const int *euid,
+                     void *stream, evx_graph **out);
+
+/* Same, from device-resident inputs (no host copy). */
+EVX_API int evx_graph_from_device(int device, int64_t num_edges, int64_t num_vertices,
+                          const int *eg_d, const int *out_v_d, const int *in_v_d,
+                          const int *out_r_d, const int *in_r_d, const int *euid_d,
+                          void *stream, evx_graph **out);
+
+EVX_API int evx_graph_free(evx_graph *g);
+EVX_API int evx_graph_info(const evx_graph *g, int64_t *num_edges, int64_t *num_vertices,
+                   int *device, int64_t *device_bytes);
+
+/* --------------------------------------------------------------- worker --
+ * Worker construction (replaces the plugin factory getWorker(int gpu),
+ * system/templates/GPUWorker/interface.snp:1-7, and the worker ctor,
+ * system/templates/GPUWorker/ctor.snp).  stream: cudaStream_t to launch on,
+ * or NULL to create one owned by the worker. */
+EVX_API int evx_worker_create(int device, void *stream, evx_worker **out);
+EVX_API int evx_worker_destroy(evx_worker *w);
+EVX_API int evx_worker_stream(evx_worker *w, void **stream);
+
+/* Bind a job (replaces DeviceJobData ctor, src/core/gpu/data.cu:496-529,
+ * MineJob, src/core/cpu/data.cc:452-466, and GPUWorker::take,
+ * system/templates/GPUWorker/take.snp).  mu/mv: k relabeled motif edges
+ * (edge 0 = (0,1); each later edge touches a mapped node; no self-loops).
+ * Roots are edge ids [beg, end); end < 0 means E-k+1.  enum_cap > 0 selects
+ * enumeration with that many rows of k ints (the YAML enumerate: <cap>).
+ * Fails with EVX_ERR_OVERFLOW if max(t) + delta overflows int32 and with
+ * EVX_ERR_NOMEM if the enumeration buffer does not fit in free memory. */
+EVX_API int evx_worker_take(evx_worker *w, const evx_graph *g, int k, const int *mu,
+                    const int *mv, int delta, int64_t beg, int64_t end,
+                    int64_t enum_cap, unsigned flags);
+
+/* Run the bound job to completion and return the count (replaces
+ * GPUWorker::run, system/templates/GPUWorker/run.snp, and the generated
+ * TMotifMatchingGPUImpl, system/templates/Impl/top.snp).  In count mode the
+ * result is the exact match count; in enumerate mode it is the number of
+ * matches found before root dispatch stopped at the cap (exact total with
+ * EVX_FLAG_EXACT_TOTAL). */
+EVX_API int evx_worker_run(evx_worker *w, uint64_t *count);
+
+/* Asynchronous form of evx_worker_run: enqueue the search on the worker's
+ * stream; evx_worker_result synchronises and returns the count. */
+EVX_API int evx_worker_launch(evx_worker *w);
+EVX_API int evx_worker_result(evx_worker *w, uint64_t *count);
+
+/* Copy min(n, rows found, cap) enumeration rows (k ints each: the original
+ * line ids of e_0..e_{k-1}) to host memory (replaces
+ * GPUWorker::printEnum, system/templates/enumerate/func.snp). */
+EVX_API int evx_worker_enum_rows(evx_worker *w, int64_t n, int *rows, int64_t *rows_written);
+
+/* Tuning knobs (autotuner): block size, blocks per SM (0 = occupancy),
+ * roots per warp fetch, steal check interval (iterations, 0 = never),
+ * minimum range width worth splitting. */
+EVX_API int evx_worker_set_tuning(evx_worker *w, int block, int blocks_per_sm,
+                          int roots_per_fetch, int steal_interval, int min_split);
+
+/* Kernel statistics of the last run: launches of this library's kernels
+ * and device milliseconds measured with CUDA events around them. */
+EVX_API int evx_worker_last_stats(evx_worker *w, int *kernel_launches, float *device_ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EVEREST_B200_H_ */

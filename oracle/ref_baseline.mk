@@ -1,0 +1,20 @@
+# Host (CPU) build of the reference's legacy Baseline search body,
+# plugins/GPUWorkerBaseline.cu lines 21-206 (binarySearchGeq, reduceEarlyIdx,
+# TMotifMatching_NextMatch, MotifMatching_dispatch), compiled where it lies in
+# the reference tree through a macro shim (ref_shim.h): __device__/__global__
+# become host functions, a loop over root ids replaces the CUDA grid, and
+# atomicAdd becomes a relaxed atomic add.  Nothing is copied into the
+# repository: the extracted lines go to $(OUT) (git-ignored) only.
+REF ?= /root/reference
+HERE := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
+OUT ?= $(HERE)_ref
+SRC := $(REF)/plugins/GPUWorkerBaseline.cu
+
+$(OUT)/libref_baseline.so: $(SRC) $(HERE)ref_shim.h $(HERE)ref_driver.cc
+	mkdir -p $(OUT)
+	sed -n '21,206p' $(SRC) > $(OUT)/baseline_body.inc
+	head -1 $(OUT)/baseline_body.inc | grep -q 'binarySearchGeq'
+	grep -q 'EXITKERNEL:' $(OUT)/baseline_body.inc
+	tail -1 $(OUT)/baseline_body.inc | grep -q '^}'
+	g++ -O3 -march=x86-64-v2 -fopenmp -fPIC -shared -std=c++17 -I$(OUT) -I$(HERE) \
+	    -o $@ $(HERE)ref_driver.cc
