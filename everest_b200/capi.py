@@ -32,7 +32,7 @@ EXPORTS = [
     "evx_graph_from_device", "evx_graph_free", "evx_graph_info", "evx_worker_create",
     "evx_worker_destroy", "evx_worker_stream", "evx_worker_take", "evx_worker_run",
     "evx_worker_launch", "evx_worker_result", "evx_worker_enum_rows", "evx_worker_set_tuning",
-    "evx_worker_last_stats",
+    "evx_worker_last_stats", "evx_host_register", "evx_host_unregister",
 ]
 
 
@@ -67,6 +67,8 @@ def lib():
             "evx_motif_parse": ([ctypes.c_char_p, _PI, _PI, _PI, _PI], _I),
             "evx_motif_parse_text": ([ctypes.c_char_p, _PI, _PI, _PI, _PI], _I),
             "evx_free": ([_P], None),
+            "evx_host_register": ([_P, _I64], _I),
+            "evx_host_unregister": ([_P], _I),
             "evx_graph_upload": ([_I, _I64, _I64, _P, _P, _P, _P, _P, _P, _P,
                                   ctypes.POINTER(_P)], _I),
             "evx_graph_from_device": ([_I, _I64, _I64, _P, _P, _P, _P, _P, _P, _P,
@@ -139,6 +141,15 @@ def edgelist_parse(path: str):
             _take_int_array(pi, E))
 
 
+def host_register(arr: np.ndarray) -> None:
+    """Page-lock a numpy array (uploads from it become async DMA)."""
+    check(lib().evx_host_register(_ptr(arr), arr.nbytes))
+
+
+def host_unregister(arr: np.ndarray) -> None:
+    check(lib().evx_host_unregister(_ptr(arr)))
+
+
 class HostGraph:
     """Host-format graph arrays (the reference's HostGraphData content)."""
 
@@ -152,6 +163,25 @@ class HostGraph:
     @property
     def total_bytes(self) -> int:
         return 24 * self.num_edges + 8 * (self.num_vertices + 1)
+
+    def arrays(self):
+        return [self.eg, self.out_v, self.in_v, self.out_r, self.in_r, self.euid]
+
+    def pin(self) -> "HostGraph":
+        """Page-lock every array (idempotent)."""
+        if not getattr(self, "_pinned", False):
+            for a in self.arrays():
+                if a.nbytes:
+                    host_register(a)
+            self._pinned = True
+        return self
+
+    def unpin(self) -> None:
+        if getattr(self, "_pinned", False):
+            for a in self.arrays():
+                if a.nbytes:
+                    host_unregister(a)
+            self._pinned = False
 
 
 def graph_build_host(u, v, t, ids=None, beg: int = 0, end: Optional[int] = None,

@@ -101,6 +101,18 @@ extern "C" {
 
 const char *evx_last_error(void) { return g_last_error.c_str(); }
 
+int evx_host_register(void *ptr, int64_t bytes) {
+  if (!ptr || bytes <= 0) return fail(EVX_ERR_INVALID, "bad host range");
+  EVX_CUDA(cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault));
+  return EVX_OK;
+}
+
+int evx_host_unregister(void *ptr) {
+  if (!ptr) return fail(EVX_ERR_INVALID, "null pointer");
+  EVX_CUDA(cudaHostUnregister(ptr));
+  return EVX_OK;
+}
+
 int evx_device_count(int *count) {
   if (!count) return fail(EVX_ERR_INVALID, "null count");
   int n = 0;
@@ -136,15 +148,15 @@ static int alloc_graph(int device, int64_t E, int64_t V, evx_graph **out, cudaSt
     if (err == cudaSuccess) { err = cudaMalloc(p, n); bytes += n; }
   };
   A((void **)&g.edges, sizeof(int4) * e1);
-  A((void **)&g.rootpos, sizeof(int2) * e1);
+  A((void **)&g.inpos, sizeof(int) * e1);
+  A((void **)&g.euid, sizeof(int) * e1);
   A((void **)&g.out_rec, sizeof(int4) * e1);
   A((void **)&g.in_rec, sizeof(int4) * e1);
-  A((void **)&g.out_off, sizeof(int) * (size_t)(V + 1));
-  A((void **)&g.in_off, sizeof(int) * (size_t)(V + 1));
+  A((void **)&g.node_rng, sizeof(int4) * (size_t)(V > 0 ? V : 1));
   g.bytes = (int64_t)bytes;
   if (err != cudaSuccess) {
-    cudaFree(g.edges); cudaFree(g.rootpos); cudaFree(g.out_rec); cudaFree(g.in_rec);
-    cudaFree(g.out_off); cudaFree(g.in_off);
+    cudaFree(g.edges); cudaFree(g.inpos); cudaFree(g.euid); cudaFree(g.out_rec);
+    cudaFree(g.in_rec); cudaFree(g.node_rng);
     delete h;
     return cuda_fail(err, "cudaMalloc(device graph)");
   }
@@ -238,8 +250,8 @@ int evx_graph_free(evx_graph *h) {
   if (!h) return EVX_OK;
   DeviceGraph &g = h->g;
   cudaSetDevice(g.device);
-  cudaFree(g.edges); cudaFree(g.rootpos); cudaFree(g.out_rec); cudaFree(g.in_rec);
-  cudaFree(g.out_off); cudaFree(g.in_off);
+  cudaFree(g.edges); cudaFree(g.inpos); cudaFree(g.euid); cudaFree(g.out_rec);
+  cudaFree(g.in_rec); cudaFree(g.node_rng);
   delete h;
   return EVX_OK;
 }

@@ -5,11 +5,9 @@
 // (include/data.h:174-186): Eg (AoS {u,v,t}), outEdgesV / inEdgesV (edge ids
 // grouped by endpoint, ascending), outEdgesR / inEdgesR (CSR offsets) and
 // Euid.  The upload moves exactly those bytes (24 E + 8 (V+1), as
-// calcTotalBytes, src/core/gpu/data.cu:22-24) and expands them on the device:
-//   edges[e]   = {u, v, t, euid}
-//   rootpos[e] = {position of e in out_rec, position of e in in_rec}
-//   out_rec[p] = {eid, v, t, position of eid in in_rec}
-//   in_rec[p]  = {eid, u, t, position of eid in out_rec}
+// calcTotalBytes, src/core/gpu/data.cu:22-24) and expands them on the device
+// into the layout described in evx_internal.cuh (16-byte adjacency records
+// carrying each edge's position in its other list, per-node int4 ranges).
 #include <climits>
 
 #include "evx_internal.cuh"
@@ -17,31 +15,41 @@
 namespace evx {
 namespace {
 
-__global__ void pack_edges_kernel(const int *__restrict__ eg, const int *__restrict__ euid,
-                                  int4 *__restrict__ edges, int n) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    edges[i] = make_int4(eg[3 * i], eg[3 * i + 1], eg[3 * i + 2], euid ? euid[i] : i);
+// positions: outpos[out_v[p]] = p, inpos[in_v[p]] = p
+__global__ void scatter_pos_kernel(const int *__restrict__ out_v, const int *__restrict__ in_v,
+                                   int *__restrict__ outpos, int *__restrict__ inpos, int n) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    outpos[out_v[p]] = p;
+    inpos[in_v[p]] = p;
   }
 }
 
-__global__ void scatter_pos_kernel(const int *__restrict__ out_v, const int *__restrict__ in_v,
-                                   int2 *__restrict__ rootpos, int n) {
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    rootpos[out_v[p]].x = p;
-    rootpos[in_v[p]].y = p;
+__global__ void pack_edges_kernel(const int *__restrict__ eg, const int *__restrict__ euid_in,
+                                  const int *__restrict__ outpos, int4 *__restrict__ edges,
+                                  int *__restrict__ euid, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    edges[i] = make_int4(eg[3 * i], eg[3 * i + 1], eg[3 * i + 2], outpos[i]);
+    euid[i] = euid_in ? euid_in[i] : i;
   }
 }
 
 __global__ void pack_rec_kernel(const int *__restrict__ out_v, const int *__restrict__ in_v,
-                                const int4 *__restrict__ edges, const int2 *__restrict__ rootpos,
+                                const int4 *__restrict__ edges, const int *__restrict__ inpos,
                                 int4 *__restrict__ out_rec, int4 *__restrict__ in_rec, int n) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
     const int eo = out_v[p];
     const int4 a = edges[eo];
-    out_rec[p] = make_int4(eo, a.y, a.z, rootpos[eo].y);
+    out_rec[p] = make_int4(eo, a.y, a.z, inpos[eo]);
     const int ei = in_v[p];
     const int4 b = edges[ei];
-    in_rec[p] = make_int4(ei, b.x, b.z, rootpos[ei].x);
+    in_rec[p] = make_int4(ei, b.x, b.z, b.w);
+  }
+}
+
+__global__ void pack_nodes_kernel(const int *__restrict__ out_r, const int *__restrict__ in_r,
+                                  int4 *__restrict__ node_rng, int nv) {
+  for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < nv; x += gridDim.x * blockDim.x) {
+    node_rng[x] = make_int4(out_r[x], out_r[x + 1], in_r[x], in_r[x + 1]);
   }
 }
 
@@ -76,13 +84,15 @@ int pack_graph(DeviceGraph &g, const int *eg_d, const int *out_v_d, const int *i
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
   const int grid = sms * 8, block = 256;
-  EVX_CUDA(cudaMemcpyAsync(g.out_off, out_r_d, sizeof(int) * (V + 1), cudaMemcpyDeviceToDevice, s));
-  EVX_CUDA(cudaMemcpyAsync(g.in_off, in_r_d, sizeof(int) * (V + 1), cudaMemcpyDeviceToDevice, s));
+  if (V > 0) pack_nodes_kernel<<<grid, block, 0, s>>>(out_r_d, in_r_d, g.node_rng, (int)V);
   if (E > 0) {
-    pack_edges_kernel<<<grid, block, 0, s>>>(eg_d, euid_d, g.edges, (int)E);
-    scatter_pos_kernel<<<grid, block, 0, s>>>(out_v_d, in_v_d, g.rootpos, (int)E);
-    pack_rec_kernel<<<grid, block, 0, s>>>(out_v_d, in_v_d, g.edges, g.rootpos, g.out_rec,
-                                           g.in_rec, (int)E);
+    int *outpos = nullptr;  // edges[].w, staged
+    EVX_CUDA(cudaMallocAsync(&outpos, sizeof(int) * (size_t)E, s));
+    scatter_pos_kernel<<<grid, block, 0, s>>>(out_v_d, in_v_d, outpos, g.inpos, (int)E);
+    pack_edges_kernel<<<grid, block, 0, s>>>(eg_d, euid_d, outpos, g.edges, g.euid, (int)E);
+    pack_rec_kernel<<<grid, block, 0, s>>>(out_v_d, in_v_d, g.edges, g.inpos, g.out_rec, g.in_rec,
+                                           (int)E);
+    EVX_CUDA(cudaFreeAsync(outpos, s));
   }
   EVX_CUDA(cudaGetLastError());
   return EVX_OK;

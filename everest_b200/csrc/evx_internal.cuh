@@ -10,18 +10,20 @@
 namespace evx {
 
 // Device layout of one graph (all int32; E < 2^31, V < 2^31).
-//   edges[e]   = {u, v, t, euid}                     root fetch + enumeration
-//   rootpos[e] = {pos of e in out_rec, pos of e in in_rec}   (absolute)
-//   out_rec[p] = {eid, v, t, pos of eid in in_rec}    grouped by u, ascending eid
-//   in_rec[p]  = {eid, u, t, pos of eid in out_rec}   grouped by v, ascending eid
-//   out_off / in_off: CSR offsets [V+1] into out_rec / in_rec.
+//   edges[e]    = {u, v, t, position of e in out_rec}     root fetch
+//   inpos[e]    = position of e in in_rec
+//   euid[e]     = original line id of e                    enumeration rows
+//   out_rec[p]  = {eid, v, t, position of eid in in_rec}   grouped by u, ascending eid
+//   in_rec[p]   = {eid, u, t, position of eid in out_rec}  grouped by v, ascending eid
+//   node_rng[x] = {out_beg, out_end, in_beg, in_end}       positions in out_rec / in_rec
+// Positions are absolute indices into out_rec / in_rec.
 struct GraphView {
   const int4 *edges;
-  const int2 *rootpos;
+  const int *inpos;
+  const int *euid;
   const int4 *out_rec;
   const int4 *in_rec;
-  const int *out_off;
-  const int *in_off;
+  const int4 *node_rng;
   int num_edges;
   int num_vertices;
 };
@@ -66,16 +68,16 @@ struct DeviceGraph {
   int64_t num_edges = 0, num_vertices = 0;
   int max_t = 0, min_t = 0;
   int4 *edges = nullptr;
-  int2 *rootpos = nullptr;
+  int *inpos = nullptr;
+  int *euid = nullptr;
   int4 *out_rec = nullptr;
   int4 *in_rec = nullptr;
-  int *out_off = nullptr;
-  int *in_off = nullptr;
+  int4 *node_rng = nullptr;
   int64_t bytes = 0;
   GraphView view() const {
     GraphView g;
-    g.edges = edges; g.rootpos = rootpos; g.out_rec = out_rec; g.in_rec = in_rec;
-    g.out_off = out_off; g.in_off = in_off;
+    g.edges = edges; g.inpos = inpos; g.euid = euid; g.out_rec = out_rec; g.in_rec = in_rec;
+    g.node_rng = node_rng;
     g.num_edges = (int)num_edges; g.num_vertices = (int)num_vertices;
     return g;
   }

@@ -13,11 +13,18 @@
 //  * adjacency entries are packed 16-byte records {eid, other, t, pos}; one
 //    ld.global.nc.v4 replaces the reference's two dependent gathers
 //    (i_S[beg] then the 12-byte AoS Eg[idx],
-//    system/templates/common/nextMatchInTask.snp:3-4);
-//  * every list opening finds its start in O(1) when the list is the
-//    previous edge's own out/in list (the record carries the edge's position
-//    in its other list), otherwise by a binary search over the records
-//    (system/templates/funcs/reduceEarlyIdx.snp);
+//    system/templates/common/nextMatchInTask.snp:3-4); per-node ranges are
+//    one int4 {out_beg, out_end, in_beg, in_end};
+//  * each lane runs its DFS as a state machine (ROOT -> OPEN -> BSEARCH ->
+//    SCAN, with pops in between) in which every iteration issues exactly one
+//    round of independent loads per lane and then does only ALU work, so the
+//    lanes of a warp overlap their memory latency even while they are in
+//    different phases (the reference executes a list opening's binary search
+//    inline, serialising the warp on it, system/templates/funcs/reduceEarlyIdx.snp);
+//  * a list opening finds its start in O(1) when the list is the previous
+//    edge's own out/in list (the record carries the edge's position in its
+//    other list), otherwise by a binary search advanced one probe per iteration;
+//  * the last level reads two records per iteration;
 //  * lanes are refilled with new roots one by one from a per-warp pool as
 //    soon as they finish (the reference refills a warp only when all 32
 //    lanes are done, system/templates/warpCentric/tidEnd.snp);
@@ -84,9 +91,12 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
   constexpr int N = K + 1;                 // motif nodes <= k + 1
   constexpr int S = (L > 1) ? (L - 1) : 1; // saved ranges for levels 0..L-2
   constexpr int KE = ENUM ? K : 1;
+  constexpr bool WIDE = !ENUM;             // two records per last-level step
+  enum : int { M_IDLE = 0, M_ROOT = 1, M_OPEN = 2, M_BS = 3, M_SCAN = 4 };
 
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
+  const int strict = args.strict_ts;
 
   int info[L];
 #pragma unroll
@@ -102,17 +112,17 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
 #pragma unroll
   for (int q = 0; q < S; q++) { sp[q] = 0; se[q] = 0; }
 
-  int level = -1;  // -1: lane idle (needs a root)
-  int pos = 0, end = 0, tl = 0;
-  int want = -1, base = 0, nmc = 0;
+  int mode = M_IDLE, level = -1;
+  int pos = 0, end = 0, bhi = 0;  // SCAN: [pos, end); BSEARCH: window [pos, bhi)
+  int tl = 0, want = -1, base = 0, nmc = 0;
   bool out = true;
   unsigned iomask = 0;
+  int key = 0, sc0 = -1, sc1 = -1, n0 = 0, n1 = -1;  // pending OPEN (n0 = root id in ROOT)
   unsigned long long cnt = 0;
 
   int pool_next = 0, pool_end = 0;
   bool exhausted = false;
   unsigned iter = 0;
-  const int strict = args.strict_ts;
 
   // (Re)derive list / target of level l from the plan, the node images and
   // the saved list choice.
@@ -126,45 +136,41 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
     else { base = (kind == 1) ? ia : ib; want = -1; }
   };
 
-  // Open the candidate list of level l given the previous matched edge.
-  auto open = [&](int l, int peid, int pt, int psrc, int pdst, int pop, int pip) {
+  // Queue the opening of level l's list after matching edge peid
+  // (t pt, endpoints psrc->pdst, positions pop in out_rec / pip in in_rec).
+  auto prepare_open = [&](int l, int peid, int pt, int psrc, int pdst, int pop, int pip) {
     const int w = sel(info, l);
     const int kind = plan_kind(w);
-    nmc = plan_nm(w);
     const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
-    int lo, hi;
+    key = strict ? pt : peid;
     if (kind == 2) {
-      const int i0 = __ldg(g.in_off + ib), i1 = __ldg(g.in_off + ib + 1);
-      const int o0 = __ldg(g.out_off + ia), o1 = __ldg(g.out_off + ia + 1);
-      if (i1 - i0 < o1 - o0) { out = false; base = ib; want = ia; lo = i0; hi = i1; }
-      else { out = true; base = ia; want = ib; lo = o0; hi = o1; }
+      n0 = ib; n1 = ia;
+      sc0 = (pdst == ib) ? pip + 1 : -1;
+      sc1 = (psrc == ia) ? pop + 1 : -1;
+    } else if (kind == 1) {
+      n0 = ia; n1 = -1;
+      sc0 = -1;
+      sc1 = (psrc == ia) ? pop + 1 : -1;
     } else {
-      out = (kind == 1);
-      base = out ? ia : ib;
-      want = -1;
-      const int *off = out ? g.out_off : g.in_off;
-      lo = __ldg(off + base);
-      hi = __ldg(off + base + 1);
+      n0 = ib; n1 = -1;
+      sc0 = (pdst == ib) ? pip + 1 : -1;
+      sc1 = -1;
     }
-    iomask = (iomask & ~(1u << l)) | ((unsigned)out << l);
-    const int4 *lst = out ? g.out_rec : g.in_rec;
-    if (strict) {
-      lo = first_t_after(lst, lo, hi, pt);
-    } else if (out && base == psrc) {
-      lo = pop + 1;
-    } else if (!out && base == pdst) {
-      lo = pip + 1;
-    } else {
-      lo = first_eid_after(lst, lo, hi, peid);
-    }
-    pos = lo;
-    end = hi;
+    mode = M_OPEN;
+  };
+
+  auto structural_ok = [&](int node) -> bool {
+    if (want >= 0) return node == want;
+    bool ok = true;
+#pragma unroll
+    for (int q = 0; q < N; q++) ok = ok && !(q < nmc && m[q] == node);
+    return ok;
   };
 
   while (true) {
     ++iter;
     // ---------------------------------------------------- root refill ----
-    unsigned idle = __ballot_sync(kFull, level < 0);
+    const unsigned idle = __ballot_sync(kFull, mode == M_IDLE);
     if (idle && !exhausted) {
       const int nidle = __popc(idle);
       const int rank = __popc(idle & lt_mask);
@@ -172,9 +178,9 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
       int nb = 0, nbe = 0;
       bool stopped = false;
       if (ENUM) {
-        int s = 0;
-        if (lane == 0) s = *(volatile int *)args.stop;
-        stopped = __shfl_sync(kFull, s, 0) != 0;
+        int sflag = 0;
+        if (lane == 0) sflag = *(volatile int *)args.stop;
+        stopped = __shfl_sync(kFull, sflag, 0) != 0;
       }
       if (stopped) {
         exhausted = true;
@@ -186,10 +192,11 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
           nb = min(got, args.root_end);
           nbe = min(got + args.roots_per_fetch, args.root_end);
         }
-        int r = -1;
-        if (level < 0) {
+        if (mode == M_IDLE) {
+          int r = -1;
           if (rank < avail) r = pool_next + rank;
           else if (nb + (rank - avail) < nbe) r = nb + (rank - avail);
+          if (r >= 0) { n0 = r; mode = M_ROOT; }
         }
         if (avail >= nidle) {
           pool_next += nidle;
@@ -198,66 +205,99 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
           pool_end = nbe;
           if (nb >= nbe) exhausted = true;
         }
-        if (r >= 0) {
-          const int4 ed = __ldg(g.edges + r);
-          if (ed.x != ed.y) {  // self-loops are not roots
-            m[0] = ed.x;
-            m[1] = ed.y;
-            tl = ed.z + args.delta;
-            if (ENUM) e[0] = r;
-            level = 0;
-            const int2 rp = __ldg(g.rootpos + r);
-            open(0, r, ed.z, ed.x, ed.y, rp.x, rp.y);
-          }
-        }
       }
     }
 
-    // -------------------------------------------------- one DFS step ----
+    // ----------------------------------------- issue this step's loads ----
+    int4 r0 = make_int4(0, 0, 0, 0), r1 = make_int4(0, 0, 0, 0);
+    int x0 = 0;
+    bool two = false;
+    {
+      const int4 *lst = out ? g.out_rec : g.in_rec;
+      if (mode == M_SCAN) {
+        r0 = __ldg(lst + pos);
+        two = WIDE && (level == L - 1) && (pos + 1 < end);
+        if (two) r1 = __ldg(lst + pos + 1);
+      } else if (mode == M_BS) {
+        const int mid = (pos + bhi) >> 1;
+        x0 = strict ? ld_t(lst + mid) : ld_eid(lst + mid);
+      } else if (mode == M_OPEN) {
+        r0 = __ldg(g.node_rng + n0);
+        if (n1 >= 0) r1 = __ldg(g.node_rng + n1);
+      } else if (mode == M_ROOT) {
+        r0 = __ldg(g.edges + n0);
+        x0 = __ldg(g.inpos + n0);
+      }
+    }
+
+    // ------------------------------------------------ process the step ----
     bool emit = false;
     int last_eid = 0;
-    if (level >= 0) {
-      if (pos < end) {
-        const int4 *lst = out ? g.out_rec : g.in_rec;
-        const int4 rc = __ldg(lst + pos);
-        ++pos;
-        if (rc.z > tl) {
-          end = pos;  // rest of the list is outside the window
+    if (mode == M_SCAN) {
+      ++pos;
+      if (r0.z > tl) {
+        pos = end;  // rest of the list is outside the window
+      } else if (structural_ok(r0.y)) {
+        if (level == L - 1) {
+          ++cnt;
+          if (ENUM) { emit = true; last_eid = r0.x; }
         } else {
-          bool ok;
-          if (want >= 0) {
-            ok = (rc.y == want);
-          } else {
-            ok = true;
-#pragma unroll
-            for (int q = 0; q < N; q++) ok = ok && !(q < nmc && m[q] == rc.y);
-          }
-          if (ok) {
-            if (level == L - 1) {
-              ++cnt;
-              if (ENUM) { emit = true; last_eid = rc.x; }
-            } else {
-              put(sp, level, pos);
-              put(se, level, end);
-              if (want < 0) put(m, nmc, rc.y);
-              if (ENUM) put(e, level + 1, rc.x);
-              const int psrc = out ? base : rc.y;
-              const int pdst = out ? rc.y : base;
-              const int pop = out ? pos - 1 : rc.w;
-              const int pip = out ? rc.w : pos - 1;
-              ++level;
-              open(level, rc.x, rc.z, psrc, pdst, pop, pip);
-            }
-          }
+          put(sp, level, pos);
+          put(se, level, end);
+          if (want < 0) put(m, nmc, r0.y);
+          if (ENUM) put(e, level + 1, r0.x);
+          const int psrc = out ? base : r0.y;
+          const int pdst = out ? r0.y : base;
+          const int pop = out ? pos - 1 : r0.w;
+          const int pip = out ? r0.w : pos - 1;
+          ++level;
+          prepare_open(level, r0.x, r0.z, psrc, pdst, pop, pip);
         }
-      } else if (level == 0) {
-        level = -1;  // root finished
-      } else {
-        --level;
-        pos = sel(sp, level);
-        end = sel(se, level);
-        restore(level);
       }
+      if (two && pos < end) {  // second record of a last-level step
+        ++pos;
+        if (r1.z > tl) pos = end;
+        else if (structural_ok(r1.y)) ++cnt;
+      }
+    } else if (mode == M_BS) {
+      const int mid = (pos + bhi) >> 1;
+      if (x0 > key) bhi = mid; else pos = mid + 1;
+      if (pos >= bhi) mode = M_SCAN;  // pos = first record after the previous edge
+    } else if (mode == M_OPEN) {
+      const int w = sel(info, level);
+      const int kind = plan_kind(w);
+      nmc = plan_nm(w);
+      const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
+      int lo, hi, sc;
+      if (kind == 2) {
+        if (r0.w - r0.z < r1.y - r1.x) { out = false; base = ib; want = ia; lo = r0.z; hi = r0.w; sc = sc0; }
+        else { out = true; base = ia; want = ib; lo = r1.x; hi = r1.y; sc = sc1; }
+      } else if (kind == 1) {
+        out = true; base = ia; want = -1; lo = r0.x; hi = r0.y; sc = sc1;
+      } else {
+        out = false; base = ib; want = -1; lo = r0.z; hi = r0.w; sc = sc0;
+      }
+      iomask = (iomask & ~(1u << level)) | ((unsigned)out << level);
+      end = hi;
+      if (!strict && sc >= 0) { pos = sc; mode = M_SCAN; }
+      else if (lo >= hi) { pos = hi; mode = M_SCAN; }
+      else { pos = lo; bhi = hi; mode = M_BS; }
+    } else if (mode == M_ROOT) {
+      if (r0.x == r0.y) {  // self-loops are not roots
+        mode = M_IDLE;
+      } else {
+        m[0] = r0.x;
+        m[1] = r0.y;
+        tl = r0.z + args.delta;
+        if (ENUM) e[0] = n0;
+        level = 0;
+        prepare_open(0, n0, r0.z, r0.x, r0.y, r0.w, x0);
+      }
+    }
+    // exhausted ranges: pop to the deepest level with work left
+    while (mode == M_SCAN && pos >= end) {
+      if (level == 0) { mode = M_IDLE; level = -1; }
+      else { --level; pos = sel(sp, level); end = sel(se, level); restore(level); }
     }
 
     // ------------------------------------------- enumeration output ----
@@ -273,8 +313,8 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
           if (slot < (unsigned long long)args.cap) {
             int *row = args.rows + slot * K;
 #pragma unroll
-            for (int q = 0; q < K - 1; q++) row[q] = __ldg(&g.edges[e[q < KE ? q : 0]].w);
-            row[K - 1] = __ldg(&g.edges[last_eid].w);
+            for (int q = 0; q < K - 1; q++) row[q] = __ldg(g.euid + e[q < KE ? q : 0]);
+            row[K - 1] = __ldg(g.euid + last_eid);
           }
           if (!args.exact_total && slot + 1 >= (unsigned long long)args.cap)
             atomicExch(args.stop, 1);
@@ -284,12 +324,12 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
 
     // ---------------------------------------- tail: finish or steal ----
     if (exhausted) {
-      const unsigned idle2 = __ballot_sync(kFull, level < 0);
+      const unsigned idle2 = __ballot_sync(kFull, mode == M_IDLE);
       if (idle2 == kFull) break;
       if (idle2 && args.steal_interval && (iter & (unsigned)(args.steal_interval - 1)) == 0) {
         // shallowest level with a splittable remaining range, then widest
         int sl = -1, sw = 0;
-        if (level >= 0) {
+        if (mode != M_IDLE) {
 #pragma unroll
           for (int l = 0; l < S; l++) {
             if (sl < 0 && l < level) {
@@ -297,20 +337,21 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
               if (w >= args.min_split) { sl = l; sw = w; }
             }
           }
-          if (sl < 0 && end - pos >= args.min_split) { sl = level; sw = end - pos; }
+          if (sl < 0 && mode == M_SCAN && end - pos >= args.min_split) { sl = level; sw = end - pos; }
         }
-        const unsigned key = sl < 0 ? 0u : (((unsigned)(L - sl) << 24) | (unsigned)min(sw, 0xFFFFFF));
-        const unsigned kmax = __reduce_max_sync(kFull, key);
+        const unsigned skey = sl < 0 ? 0u : (((unsigned)(L - sl) << 24) | (unsigned)min(sw, 0xFFFFFF));
+        const unsigned kmax = __reduce_max_sync(kFull, skey);
         if (kmax) {
-          const int donor = __ffs(__ballot_sync(kFull, key == kmax)) - 1;
+          const int donor = __ffs(__ballot_sync(kFull, skey == kmax)) - 1;
           const int split_l = L - (int)(kmax >> 24);
           int p0 = 0, p1 = 0;
           if (lane == donor) {
-            p0 = (split_l == level) ? pos : sel(sp, split_l);
-            p1 = (split_l == level) ? end : sel(se, split_l);
+            const bool cur = (split_l == level);
+            p0 = cur ? pos : sel(sp, split_l);
+            p1 = cur ? end : sel(se, split_l);
             const bool o = (iomask >> split_l) & 1u;
             p1 = first_t_after(o ? g.out_rec : g.in_rec, p0, p1, tl);  // window end
-            if (split_l == level) end = p1; else put(se, split_l, p1);
+            if (cur) end = p1; else put(se, split_l, p1);
           }
           p0 = __shfl_sync(kFull, p0, donor);
           p1 = __shfl_sync(kFull, p1, donor);
@@ -319,7 +360,7 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
           if (nthief > 0) {
             const int parts = nthief + 1;
             const int rank = __popc(idle2 & lt_mask);
-            const bool thief = (level < 0) && rank < nthief;
+            const bool thief = (mode == M_IDLE) && rank < nthief;
 #pragma unroll
             for (int q = 0; q < N; q++) {
               const int x = __shfl_sync(kFull, m[q], donor);
@@ -338,6 +379,7 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
               tl = dtl;
               iomask = dio;
               level = split_l;
+              mode = M_SCAN;
               pos = p0 + (int)((long long)w * (rank + 1) / parts);
               end = p0 + (int)((long long)w * (rank + 2) / parts);
 #pragma unroll
@@ -347,6 +389,12 @@ search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
             if (lane == donor) {
               const int ne = p0 + (int)((long long)w / parts);
               if (split_l == level) end = ne; else put(se, split_l, ne);
+            }
+          } else if (lane == donor) {
+            // nothing to split after trimming: drop an exhausted range
+            while (mode == M_SCAN && pos >= end) {
+              if (level == 0) { mode = M_IDLE; level = -1; }
+              else { --level; pos = sel(sp, level); end = sel(se, level); restore(level); }
             }
           }
         }

@@ -84,6 +84,11 @@ EVX_API int evx_motif_parse_text(const char *text, int *k, int *mu, int *mv, int
 
 EVX_API void evx_free(void *p);
 
+/* Page-lock host memory so uploads from it run as asynchronous DMA
+ * (cudaHostRegister / cudaHostUnregister). */
+EVX_API int evx_host_register(void *ptr, int64_t bytes);
+EVX_API int evx_host_unregister(void *ptr);
+
 /* --------------------------------------------------------- device graph --
  * Allocation + host->device transfer of one graph (replaces
  * GraphDataManager::alloc / moveAsync / waitMove,
