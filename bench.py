@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--impl", default="evx", choices=["evx", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--single-query", type=int, default=-1,
+                    help="profiling aid: run only query I of the workload --reps times and exit")
+    ap.add_argument("--reps", type=int, default=2)
     return ap.parse_args()
 
 
@@ -352,8 +355,28 @@ def run_gpu_arm(args):
     return 0
 
 
+def run_single_query(args):
+    """Run one query of the workload a few times on cuda:0 (for ncu captures)."""
+    from everest_b200 import capi, synth, workloads
+    stats = workload_stats(args.workload)
+    spec = synth.SPECS[stats["graph"]]
+    q = workloads.queries(args.workload)[args.single_query]
+    u, v, t = synth.load_or_generate(spec.name)
+    dg = capi.DeviceGraph(capi.graph_build_host(u, v, t), 0)
+    w = capi.Worker(0)
+    for _ in range(args.reps):
+        w.take(dg, q["mu"], q["mv"], q["delta"])
+        c = w.run()
+        print(json.dumps({"query": q["name"], "count": c, **w.last_stats()}), flush=True)
+    w.close()
+    dg.free()
+    return 0
+
+
 def main():
     args = parse()
+    if args.single_query >= 0:
+        return run_single_query(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)

@@ -23,6 +23,7 @@ EVX_ERR = {
 FLAG_STRICT_TS = 1
 FLAG_EXACT_TOTAL = 2
 FLAG_NO_STEAL = 4
+FLAG_NO_PAIR_INDEX = 8
 MAX_MOTIF_EDGES = 8
 
 # every symbol include/everest_b200.h declares

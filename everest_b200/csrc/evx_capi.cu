@@ -170,6 +170,10 @@ static int finish_graph(evx_graph *h, cudaStream_t s) {
   EVX_CUDA(cudaMalloc(&scratch, 2 * sizeof(int)));
   int rc = graph_t_range(h->g, scratch, s);
   cudaFree(scratch);
+  if (!rc) rc = build_pair_index(h->g, s);
+  if (!rc) {
+    EVX_CUDA(cudaStreamSynchronize(s));
+  }
   return rc;
 }
 
@@ -251,7 +255,7 @@ int evx_graph_free(evx_graph *h) {
   DeviceGraph &g = h->g;
   cudaSetDevice(g.device);
   cudaFree(g.edges); cudaFree(g.inpos); cudaFree(g.euid); cudaFree(g.out_rec);
-  cudaFree(g.in_rec); cudaFree(g.node_rng);
+  cudaFree(g.in_rec); cudaFree(g.node_rng); cudaFree(g.pair_tab); cudaFree(g.pair_rec);
   delete h;
   return EVX_OK;
 }
@@ -381,6 +385,16 @@ int evx_worker_take(evx_worker *w, const evx_graph *gh, int k, const int *mu, co
   a.steal_interval = (flags & EVX_FLAG_NO_STEAL) ? 0 : w->steal_interval;
   a.min_split = w->min_split;
   a.enumerate = enum_cap > 0 ? 1 : 0;
+  {
+    // Range arithmetic on the pair index for the last edge when it closes
+    // on two nodes mapped before the second-to-last edge (its pair is then
+    // fixed per partial match); for k == 2 the root maps both.
+    const int wl = plan.info[k - 2];
+    const int nm_prev = (k >= 3) ? plan_nm(plan.info[k - 3]) : 2;
+    const bool fixed_pair = plan_a(wl) < nm_prev && plan_b(wl) < nm_prev;
+    a.inline_last = (enum_cap <= 0 && !(flags & EVX_FLAG_NO_PAIR_INDEX) && plan_kind(wl) == 2 &&
+                     fixed_pair) ? 1 : 0;
+  }
   a.exact_total = (flags & EVX_FLAG_EXACT_TOTAL) ? 1 : 0;
   a.cap = enum_cap;
   a.rows = w->rows_d;

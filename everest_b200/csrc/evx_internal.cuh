@@ -16,6 +16,9 @@ namespace evx {
 //   out_rec[p]  = {eid, v, t, position of eid in in_rec}   grouped by u, ascending eid
 //   in_rec[p]   = {eid, u, t, position of eid in out_rec}  grouped by v, ascending eid
 //   node_rng[x] = {out_beg, out_end, in_beg, in_end}       positions in out_rec / in_rec
+//   pair_rec[i] = {eid, t} grouped by static edge (u, v), ascending eid
+//   pair_tab[h] = {v, u, start, len}: open-addressing table (u, v) -> run in pair_rec
+//                 (the first 8 bytes hold the 64-bit key; all ones = empty)
 // Positions are absolute indices into out_rec / in_rec.
 struct GraphView {
   const int4 *edges;
@@ -24,9 +27,27 @@ struct GraphView {
   const int4 *out_rec;
   const int4 *in_rec;
   const int4 *node_rng;
+  const int4 *pair_tab;
+  const int2 *pair_rec;
+  unsigned long long pair_mask;
+  int pair_max_probe;
   int num_edges;
   int num_vertices;
 };
+
+__host__ __device__ inline unsigned long long pair_key(int u, int v) {
+  return ((unsigned long long)(unsigned)u << 32) | (unsigned long long)(unsigned)v;
+}
+
+// 64-bit finalizer (splitmix64 constants) used as the pair-table hash.
+__host__ __device__ inline unsigned long long pair_hash(unsigned long long x) {
+  x ^= x >> 30;
+  x *= 0xbf58476d1ce4e5b9ull;
+  x ^= x >> 27;
+  x *= 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return x;
+}
 
 // Per-level search plan.  Level l (0-based) matches motif edge j = l + 1.
 //   kind 0: new source -> scan in-list of image(b)
@@ -54,6 +75,7 @@ struct SearchArgs {
   int steal_interval;         // iterations between steal checks (power of 2), 0 = off
   int min_split;              // smallest range width worth splitting
   int enumerate;              // 1: write rows
+  int inline_last;            // count a closing last edge by range arithmetic on the pair index
   int exact_total;            // enumerate: keep counting past the cap
   long long cap;              // enumeration rows capacity
   int *rows;                  // [cap * k] original line ids
@@ -73,11 +95,17 @@ struct DeviceGraph {
   int4 *out_rec = nullptr;
   int4 *in_rec = nullptr;
   int4 *node_rng = nullptr;
+  int4 *pair_tab = nullptr;
+  int2 *pair_rec = nullptr;
+  unsigned long long pair_mask = 0;
+  int pair_max_probe = 0;
   int64_t bytes = 0;
   GraphView view() const {
     GraphView g;
     g.edges = edges; g.inpos = inpos; g.euid = euid; g.out_rec = out_rec; g.in_rec = in_rec;
     g.node_rng = node_rng;
+    g.pair_tab = pair_tab; g.pair_rec = pair_rec; g.pair_mask = pair_mask;
+    g.pair_max_probe = pair_max_probe;
     g.num_edges = (int)num_edges; g.num_vertices = (int)num_vertices;
     return g;
   }
@@ -99,6 +127,9 @@ int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &a
                   int grid, int block, cudaStream_t stream);
 // Max resident blocks per SM for a given motif size / mode / block.
 int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm);
+
+// Build the pair index (defined in evx_pairs.cu); needs edges[] packed.
+int build_pair_index(DeviceGraph &g, cudaStream_t s);
 
 // Build the packed device layout from the uploaded host-format arrays
 // (defined in evx_graph.cu).

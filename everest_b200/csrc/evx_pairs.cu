@@ -1,0 +1,167 @@
+// Pair index: for every static edge (u, v) the run of its temporal edges
+// {eid, t}, ascending in eid, plus an open-addressing hash table
+// (u, v) -> (start, len).  It lets the search count a closing last motif
+// edge by range arithmetic (the number of u->v edges with id after the
+// previous edge and t <= t(e_0) + delta) instead of scanning a list.
+//
+// Built on the device from the packed edge array: a stable 64-bit radix sort
+// of (u, v) keys with edge-id values (CUB), run-length encoding of the sorted
+// keys, and a parallel hash insert (atomicCAS on the 64-bit key).
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_run_length_encode.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include "evx_internal.cuh"
+
+namespace evx {
+namespace {
+
+__global__ void pair_keys_kernel(const int4 *__restrict__ edges, unsigned long long *__restrict__ keys,
+                                 int *__restrict__ vals, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int4 e = edges[i];
+    keys[i] = pair_key(e.x, e.y);
+    vals[i] = i;
+  }
+}
+
+__global__ void pair_rec_kernel(const int *__restrict__ eids, const int4 *__restrict__ edges,
+                                int2 *__restrict__ rec, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int e = eids[i];
+    rec[i] = make_int2(e, edges[e].z);
+  }
+}
+
+__global__ void pair_clear_kernel(int4 *__restrict__ tab, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    tab[i] = make_int4(-1, -1, 0, 0);
+}
+
+// Insert every run; the probe sequence is bounded by the table size, and the
+// longest probe actually used is recorded so lookups can stop there.
+__global__ void pair_insert_kernel(const unsigned long long *__restrict__ ukeys,
+                                   const int *__restrict__ starts, const int *__restrict__ lens,
+                                   const int *__restrict__ num_runs, int4 *__restrict__ tab,
+                                   unsigned long long mask, int *__restrict__ max_probe,
+                                   int *__restrict__ overflow) {
+  const int P = *num_runs;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    const unsigned long long key = ukeys[p];
+    unsigned long long h = pair_hash(key) & mask;
+    bool done = false;
+    for (unsigned long long i = 0; i <= mask; i++) {
+      unsigned long long *slot = reinterpret_cast<unsigned long long *>(tab + h);
+      const unsigned long long prev = atomicCAS(slot, ~0ull, key);
+      if (prev == ~0ull) {
+        tab[h].z = starts[p];
+        tab[h].w = lens[p];
+        atomicMax(max_probe, (int)i + 1);
+        done = true;
+        break;
+      }
+      h = (h + 1) & mask;
+    }
+    if (!done) atomicExch(overflow, 1);
+  }
+}
+
+}  // namespace
+
+int build_pair_index(DeviceGraph &g, cudaStream_t s) {
+  const int64_t E = g.num_edges;
+  if (E <= 0) {
+    g.pair_mask = 0;
+    g.pair_max_probe = 0;
+    EVX_CUDA(cudaMalloc(&g.pair_tab, sizeof(int4)));
+    EVX_CUDA(cudaMalloc(&g.pair_rec, sizeof(int2)));
+    EVX_CUDA(cudaMemsetAsync(g.pair_tab, 0xff, sizeof(int4), s));
+    g.bytes += sizeof(int4) + sizeof(int2);
+    return EVX_OK;
+  }
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
+  const int grid = sms * 8, block = 256;
+  const int n = (int)E;
+  unsigned long long *keys = nullptr, *keys_sorted = nullptr, *ukeys = nullptr;
+  int *vals = nullptr, *vals_sorted = nullptr, *lens = nullptr, *starts = nullptr, *ctr = nullptr;
+  void *tmp = nullptr;
+  size_t tmp_bytes = 0, t1 = 0, t2 = 0, t3 = 0;
+  int rc = EVX_OK;
+  auto A = [&](void **p, size_t b) {
+    if (rc == EVX_OK) {
+      cudaError_t e = cudaMallocAsync(p, b, s);
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaMallocAsync(pair index scratch)");
+    }
+  };
+  A((void **)&keys, sizeof(unsigned long long) * n);
+  A((void **)&keys_sorted, sizeof(unsigned long long) * n);
+  A((void **)&ukeys, sizeof(unsigned long long) * n);
+  A((void **)&vals, sizeof(int) * n);
+  A((void **)&vals_sorted, sizeof(int) * n);
+  A((void **)&lens, sizeof(int) * n);
+  A((void **)&starts, sizeof(int) * n);
+  A((void **)&ctr, sizeof(int) * 4);  // [0] runs, [1] max probe, [2] overflow
+  if (rc) goto cleanup;
+  // key bits actually used: u and v < V
+  {
+    int vb = 1;
+    while ((1ll << vb) < g.num_vertices + 1 && vb < 31) vb++;
+    const int end_bit = 32 + vb;
+    cub::DeviceRadixSort::SortPairs(nullptr, t1, keys, keys_sorted, vals, vals_sorted, n, 0, end_bit, s);
+    cub::DeviceRunLengthEncode::Encode(nullptr, t2, keys_sorted, ukeys, lens, ctr, n, s);
+    cub::DeviceScan::ExclusiveSum(nullptr, t3, lens, starts, n, s);
+    tmp_bytes = t1 > t2 ? t1 : t2;
+    tmp_bytes = tmp_bytes > t3 ? tmp_bytes : t3;
+    A(&tmp, tmp_bytes);
+    if (rc) goto cleanup;
+    EVX_CUDA(cudaMemsetAsync(lens, 0, sizeof(int) * n, s));
+    pair_keys_kernel<<<grid, block, 0, s>>>(g.edges, keys, vals, n);
+    cub::DeviceRadixSort::SortPairs(tmp, t1, keys, keys_sorted, vals, vals_sorted, n, 0, end_bit, s);
+    cub::DeviceRunLengthEncode::Encode(tmp, t2, keys_sorted, ukeys, lens, ctr, n, s);
+    // lens beyond the run count are never read by the scan's consumers; the
+    // scan runs over n entries and only the first 'runs' starts are used
+    cub::DeviceScan::ExclusiveSum(tmp, t3, lens, starts, n, s);
+  }
+  {
+    int runs = 0;
+    EVX_CUDA(cudaMemcpyAsync(&runs, ctr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    EVX_CUDA(cudaStreamSynchronize(s));
+    long long cap = 1;
+    while (cap < 2ll * runs + 2) cap <<= 1;
+    g.pair_mask = (unsigned long long)(cap - 1);
+    cudaError_t e = cudaMalloc(&g.pair_tab, sizeof(int4) * (size_t)cap);
+    if (e == cudaSuccess) e = cudaMalloc(&g.pair_rec, sizeof(int2) * (size_t)n);
+    if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMalloc(pair index)"); goto cleanup; }
+    g.bytes += (int64_t)(sizeof(int4) * cap + sizeof(int2) * n);
+    EVX_CUDA(cudaMemsetAsync(ctr + 1, 0, 2 * sizeof(int), s));
+    pair_clear_kernel<<<grid, block, 0, s>>>(g.pair_tab, cap);
+    pair_rec_kernel<<<grid, block, 0, s>>>(vals_sorted, g.edges, g.pair_rec, n);
+    pair_insert_kernel<<<grid, block, 0, s>>>(ukeys, starts, lens, ctr, g.pair_tab, g.pair_mask, ctr + 1,
+                                              ctr + 2);
+    int h[2] = {0, 0};
+    EVX_CUDA(cudaGetLastError());
+    EVX_CUDA(cudaMemcpyAsync(h, ctr + 1, sizeof(h), cudaMemcpyDeviceToHost, s));
+    EVX_CUDA(cudaStreamSynchronize(s));
+    if (h[1]) { rc = fail(EVX_ERR_CUDA, "pair index insert overflow"); goto cleanup; }
+    g.pair_max_probe = h[0];
+  }
+cleanup:
+  cudaFreeAsync(keys, s);
+  cudaFreeAsync(keys_sorted, s);
+  cudaFreeAsync(ukeys, s);
+  cudaFreeAsync(vals, s);
+  cudaFreeAsync(vals_sorted, s);
+  cudaFreeAsync(lens, s);
+  cudaFreeAsync(starts, s);
+  cudaFreeAsync(ctr, s);
+  if (tmp) cudaFreeAsync(tmp, s);
+  if (rc == EVX_OK) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = cuda_fail(e, "pair index build");
+  }
+  return rc;
+}
+
+}  // namespace evx

@@ -7,35 +7,33 @@
 // nodes to graph nodes.  Motif edge j >= 1 is searched in the out-list of the
 // image of its source when its target is new, the in-list of the image of its
 // target when its source is new, and the shorter of the two when both are
-// mapped (system/templates/common/resolveMi.snp:1-28).
+// mapped (system/templates/common/resolveMi.snp:1-28).  Candidates start
+// after the previous edge's id (system/templates/funcs/reduceEarlyIdx.snp)
+// and stop at the first t > t(e_0) + delta
+// (system/templates/common/nextMatchInTask.snp:1-21).
 //
 // B200 design (not a translation of the reference's per-lane register DFS):
-//  * adjacency entries are packed 16-byte records {eid, other, t, pos}; one
+//  * warp-synchronous levels: all 32 lanes of a warp work on the same motif
+//    level at once, each on its own partial match, so every load and compare
+//    is issued for the whole warp.  A level's matches become child tasks in
+//    a per-warp shared-memory buffer (32-byte records with a parent link);
+//    whenever 32 are queued the warp descends, processes them as one batch,
+//    and returns (depth-first over batches, bounded buffers);
+//  * adjacency entries are packed 16-byte records {eid, other, t, pos}: one
 //    ld.global.nc.v4 replaces the reference's two dependent gathers
-//    (i_S[beg] then the 12-byte AoS Eg[idx],
-//    system/templates/common/nextMatchInTask.snp:3-4); per-node ranges are
+//    (system/templates/common/nextMatchInTask.snp:3-4); per-node ranges are
 //    one int4 {out_beg, out_end, in_beg, in_end};
-//  * each lane runs its DFS as a state machine (ROOT -> OPEN -> BSEARCH ->
-//    SCAN, with pops in between) in which every iteration issues exactly one
-//    round of independent loads per lane and then does only ALU work, so the
-//    lanes of a warp overlap their memory latency even while they are in
-//    different phases (the reference executes a list opening's binary search
-//    inline, serialising the warp on it, system/templates/funcs/reduceEarlyIdx.snp);
 //  * a list opening finds its start in O(1) when the list is the previous
 //    edge's own out/in list (the record carries the edge's position in its
-//    other list), otherwise by a binary search advanced one probe per iteration;
-//  * the last level reads two records per iteration;
-//  * lanes are refilled with new roots one by one from a per-warp pool as
-//    soon as they finish (the reference refills a warp only when all 32
-//    lanes are done, system/templates/warpCentric/tidEnd.snp);
-//  * when the global root cursor is exhausted, idle lanes split the
-//    shallowest, widest remaining candidate range of one donor lane into
-//    equal contiguous parts (warp shuffle of the donor state, exact
-//    partition), in place of the reference's one-candidate-per-thief split
-//    (system/templates/warpBalancing/top.snp) and its host-driven
-//    dump/expand rounds (system/templates/tailExpan/Expanding.snp);
+//    other list), otherwise by a warp-converged binary search;
+//  * when some lanes of a level run dry, idle lanes take equal contiguous
+//    slices of the widest remaining candidate range of that level (one warp
+//    shuffle of the donor's state; an exact partition), in place of the
+//    reference's one-candidate-per-thief split (system/templates/warpBalancing/top.snp)
+//    and its host-driven dump/expand rounds (system/templates/tailExpan/Expanding.snp);
+//  * the last level reads several records per lane per step (count mode);
 //  * enumeration slots are reserved with one warp-aggregated atomicAdd per
-//    iteration (the reference issues one atomicAdd per match,
+//    step (the reference issues one atomicAdd per match,
 //    system/tmine/KernelGen.py:505-524).
 #include "evx_internal.cuh"
 
@@ -43,6 +41,9 @@ namespace evx {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kCap = 64;        // task slots per buffered level per warp
+constexpr int kBlock = 128;     // threads per block
+constexpr int kWarps = kBlock / 32;
 
 template <int N>
 __device__ __forceinline__ int sel(const int (&a)[N], int i) {
@@ -62,19 +63,6 @@ __device__ __forceinline__ void put(int (&a)[N], int i, int v) {
 __device__ __forceinline__ int ld_eid(const int4 *p) { return __ldg(&p->x); }
 __device__ __forceinline__ int ld_t(const int4 *p) { return __ldg(&p->z); }
 
-// First position in [lo, hi) whose edge id is greater than prev.
-__device__ __forceinline__ int first_eid_after(const int4 *lst, int lo, int hi, int prev) {
-  if (lo >= hi) return hi;
-  if (ld_eid(lst + hi - 1) <= prev) return hi;
-  if (ld_eid(lst + lo) > prev) return lo;
-  int a = lo + 1, b = hi - 1;  // eid(b) > prev, eid(lo) <= prev
-  while (a < b) {
-    int mid = (a + b) >> 1;
-    if (ld_eid(lst + mid) > prev) b = mid; else a = mid + 1;
-  }
-  return a;
-}
-
 // First position in [lo, hi) whose timestamp is greater than tv.
 __device__ __forceinline__ int first_t_after(const int4 *lst, int lo, int hi, int tv) {
   while (lo < hi) {
@@ -84,341 +72,512 @@ __device__ __forceinline__ int first_t_after(const int4 *lst, int lo, int hi, in
   return lo;
 }
 
+// (start, len) of the run of u->v edges in pair_rec; len 0 when absent.  The
+// probe sequence stops at the longest one the table build used.
+__device__ __forceinline__ int2 pair_find(const GraphView &g, int u, int v) {
+  const unsigned long long key = pair_key(u, v);
+  unsigned long long h = pair_hash(key) & g.pair_mask;
+  for (int i = 0; i < g.pair_max_probe; i++) {
+    const int4 s = __ldg(g.pair_tab + h);
+    const unsigned long long k = ((unsigned long long)(unsigned)s.y << 32) | (unsigned)s.x;
+    if (k == key) return make_int2(s.z, s.w);
+    if (k == ~0ull) break;
+    h = (h + 1) & g.pair_mask;
+  }
+  return make_int2(0, 0);
+}
+
+// First index in [lo, hi) of pair_rec whose timestamp is greater than tl.
+__device__ __forceinline__ int pair_first_t_after(const GraphView &g, int lo, int hi, int tl) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(&g.pair_rec[mid].y) > tl) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+// First index in [lo, hi) of pair_rec whose edge id (timestamp in strict
+// mode) is greater than key.
+__device__ __forceinline__ int pair_first_key_after(const GraphView &g, int lo, int hi, int key,
+                                                    bool strict) {
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const int2 r = __ldg(g.pair_rec + mid);
+    if ((strict ? r.y : r.x) > key) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+// Entries of the run [start, start + len) after the previous edge (edge id >
+// key; timestamp > key in strict mode) and inside the window (t <= tl).
+__device__ __forceinline__ int pair_window(const GraphView &g, int start, int len, int key, int tl,
+                                           bool strict) {
+  if (len <= 0) return 0;
+  if (len <= 4) {
+    int2 r[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (q < len) r[q] = __ldg(g.pair_rec + start + q);
+    int c = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if (q < len) c += ((strict ? r[q].y : r[q].x) > key && r[q].y <= tl) ? 1 : 0;
+    return c;
+  }
+  int a = start, b = start + len;
+  while (a < b) {
+    const int mid = (a + b) >> 1;
+    const int2 r = __ldg(g.pair_rec + mid);
+    if ((strict ? r.y : r.x) > key) b = mid; else a = mid + 1;
+  }
+  int c = a, d = start + len;
+  while (c < d) {
+    const int mid = (c + d) >> 1;
+    if (__ldg(&g.pair_rec[mid].y) > tl) d = mid; else c = mid + 1;
+  }
+  return c - a;
+}
+
+// Per-warp shared state.
+//   root[r]           = {u, v, tl, e0} of the batch's root on lane r
+//   task[l-1][s][0/1] = {parent, src, dst, eid}, {t, pos in out_rec, pos in in_rec, root}
+//                       of a partial match waiting at level l (l = 1 .. k-2)
+//   save[l][lane]     = scan state of level l parked while the warp descends
+template <int K>
+struct alignas(16) WarpSmem {
+  int4 root[32];
+  int4 task[(K > 2) ? (K - 2) : 1][kCap][2];
+  int4 save[(K > 2) ? (K - 2) : 1][32][2];
+  int nb[K];
+};
+
+// The previous matched edge of a task (what the next list opening needs).
+struct Prev {
+  int eid, t, src, dst, pop, pip;
+};
+
 template <int K, bool ENUM>
-__global__ void __launch_bounds__(256)
-search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
-  constexpr int L = K - 1;                 // search levels (motif edges 1..k-1)
-  constexpr int N = K + 1;                 // motif nodes <= k + 1
-  constexpr int S = (L > 1) ? (L - 1) : 1; // saved ranges for levels 0..L-2
-  constexpr int KE = ENUM ? K : 1;
-  constexpr bool WIDE = !ENUM;             // two records per last-level step
-  enum : int { M_IDLE = 0, M_ROOT = 1, M_OPEN = 2, M_BS = 3, M_SCAN = 4 };
+struct Searcher {
+  static constexpr int L = K - 1;          // levels; level l opens motif edge l + 1
+  static constexpr int N = K + 1;          // motif nodes <= k + 1
+  static constexpr int KE = ENUM ? K : 1;
+  static constexpr int WIDE = ENUM ? 1 : 4;  // records per lane per last-level step
 
-  const int lane = threadIdx.x & 31;
-  const unsigned lt_mask = (1u << lane) - 1u;
-  const int strict = args.strict_ts;
+  const GraphView &g;
+  const MotifPlan &plan;
+  const SearchArgs &args;
+  WarpSmem<K> &sm;
+  const int lane;
+  const unsigned lt;
+  const int strict;
+  unsigned long long cnt;
 
-  int info[L];
+  __device__ Searcher(const GraphView &g_, const MotifPlan &p_, const SearchArgs &a_, WarpSmem<K> &s_,
+                      int lane_)
+      : g(g_), plan(p_), args(a_), sm(s_), lane(lane_), lt((1u << lane_) - 1u),
+        strict(a_.strict_ts), cnt(0) {}
+
+  // Node images and edge ids of the partial match in slot s of level l.
+  template <int l>
+  __device__ __forceinline__ void reconstruct(int s, int (&m)[N], int (&e)[KE], Prev &p, int &root) {
 #pragma unroll
-  for (int l = 0; l < L; l++) info[l] = plan.info[l];
-
-  int m[N];
-#pragma unroll
-  for (int q = 0; q < N; q++) m[q] = -1;
-  int e[KE];
-#pragma unroll
-  for (int q = 0; q < KE; q++) e[q] = 0;
-  int sp[S], se[S];
-#pragma unroll
-  for (int q = 0; q < S; q++) { sp[q] = 0; se[q] = 0; }
-
-  int mode = M_IDLE, level = -1;
-  int pos = 0, end = 0, bhi = 0;  // SCAN: [pos, end); BSEARCH: window [pos, bhi)
-  int tl = 0, want = -1, base = 0, nmc = 0;
-  bool out = true;
-  unsigned iomask = 0;
-  int key = 0, sc0 = -1, sc1 = -1, n0 = 0, n1 = -1;  // pending OPEN (n0 = root id in ROOT)
-  unsigned long long cnt = 0;
-
-  int pool_next = 0, pool_end = 0;
-  bool exhausted = false;
-  unsigned iter = 0;
-
-  // (Re)derive list / target of level l from the plan, the node images and
-  // the saved list choice.
-  auto restore = [&](int l) {
-    const int w = sel(info, l);
-    const int kind = plan_kind(w);
-    nmc = plan_nm(w);
-    out = (iomask >> l) & 1u;
-    const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
-    if (kind == 2) { base = out ? ia : ib; want = out ? ib : ia; }
-    else { base = (kind == 1) ? ia : ib; want = -1; }
-  };
-
-  // Queue the opening of level l's list after matching edge peid
-  // (t pt, endpoints psrc->pdst, positions pop in out_rec / pip in in_rec).
-  auto prepare_open = [&](int l, int peid, int pt, int psrc, int pdst, int pop, int pip) {
-    const int w = sel(info, l);
-    const int kind = plan_kind(w);
-    const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
-    key = strict ? pt : peid;
-    if (kind == 2) {
-      n0 = ib; n1 = ia;
-      sc0 = (pdst == ib) ? pip + 1 : -1;
-      sc1 = (psrc == ia) ? pop + 1 : -1;
-    } else if (kind == 1) {
-      n0 = ia; n1 = -1;
-      sc0 = -1;
-      sc1 = (psrc == ia) ? pop + 1 : -1;
+    for (int q = 0; q < N; q++) m[q] = -1;
+    if constexpr (l == 0) {
+      root = s;
     } else {
-      n0 = ib; n1 = -1;
-      sc0 = (pdst == ib) ? pip + 1 : -1;
-      sc1 = -1;
+      const int4 a0 = sm.task[l - 1][s][0], a1 = sm.task[l - 1][s][1];
+      p.eid = a0.w; p.t = a1.x; p.src = a0.y; p.dst = a0.z; p.pop = a1.y; p.pip = a1.z;
+      root = a1.w;
+      int cur = s;
+#pragma unroll
+      for (int j = l; j >= 1; j--) {
+        const int4 t0 = sm.task[j - 1][cur][0];
+        const int w = plan.info[j - 1];  // level j-1 matched motif edge j
+        const int kind = plan_kind(w);
+        if (kind == 0) put(m, plan_nm(w), t0.y);
+        else if (kind == 1) put(m, plan_nm(w), t0.z);
+        if (ENUM) put(e, j, t0.w);
+        cur = t0.x;
+      }
     }
-    mode = M_OPEN;
-  };
+    const int4 r = sm.root[root];
+    m[0] = r.x;
+    m[1] = r.y;
+    if (ENUM) e[0] = r.w;
+    if constexpr (l == 0) {
+      (void)p;
+    }
+  }
 
-  auto structural_ok = [&](int node) -> bool {
+  __device__ __forceinline__ bool structural_ok(int node, int want, int nmc, const int (&m)[N]) const {
     if (want >= 0) return node == want;
     bool ok = true;
 #pragma unroll
     for (int q = 0; q < N; q++) ok = ok && !(q < nmc && m[q] == node);
     return ok;
-  };
+  }
 
-  while (true) {
-    ++iter;
-    // ---------------------------------------------------- root refill ----
-    const unsigned idle = __ballot_sync(kFull, mode == M_IDLE);
-    if (idle && !exhausted) {
-      const int nidle = __popc(idle);
-      const int rank = __popc(idle & lt_mask);
-      const int avail = pool_end - pool_next;
-      int nb = 0, nbe = 0;
-      bool stopped = false;
-      if (ENUM) {
-        int sflag = 0;
-        if (lane == 0) sflag = *(volatile int *)args.stop;
-        stopped = __shfl_sync(kFull, sflag, 0) != 0;
-      }
-      if (stopped) {
-        exhausted = true;
-      } else {
-        if (avail < nidle) {
-          int got = 0;
-          if (lane == 0) got = atomicAdd(args.cursor, args.roots_per_fetch);
-          got = __shfl_sync(kFull, got, 0);
-          nb = min(got, args.root_end);
-          nbe = min(got + args.roots_per_fetch, args.root_end);
-        }
-        if (mode == M_IDLE) {
-          int r = -1;
-          if (rank < avail) r = pool_next + rank;
-          else if (nb + (rank - avail) < nbe) r = nb + (rank - avail);
-          if (r >= 0) { n0 = r; mode = M_ROOT; }
-        }
-        if (avail >= nidle) {
-          pool_next += nidle;
-        } else {
-          pool_next = min(nb + (nidle - avail), nbe);
-          pool_end = nbe;
-          if (nb >= nbe) exhausted = true;
-        }
+  // Push one child partial match (found at level l) into level l+1's buffer.
+  template <int l>
+  __device__ __forceinline__ void push_children(bool push, int parent, const int4 &rc, bool out, int base,
+                                                int pos_found, int root) {
+    const unsigned pm = __ballot_sync(kFull, push);
+    if (!pm) return;
+    const int nb = sm.nb[l + 1];
+    if (push) {
+      const int s = nb + __popc(pm & lt);
+      const int src = out ? base : rc.y, dst = out ? rc.y : base;
+      const int pop = out ? pos_found : rc.w, pip = out ? rc.w : pos_found;
+      sm.task[l][s][0] = make_int4(parent, src, dst, rc.x);
+      sm.task[l][s][1] = make_int4(rc.z, pop, pip, root);
+    }
+    __syncwarp();
+    if (lane == 0) sm.nb[l + 1] = nb + __popc(pm);
+    __syncwarp();
+  }
+
+  // Process one queued batch (up to 32 tasks) of level l+1, then move the
+  // tasks that were not in the batch to the front of the buffer.
+  template <int l>
+  __device__ __forceinline__ void descend() {
+    if constexpr (l + 1 < L) {
+      const int nb = sm.nb[l + 1];
+      const int take = nb < 32 ? nb : 32;
+      level<l + 1>(lane < take, lane, take);
+      __syncwarp();
+      const int rest = sm.nb[l + 1] - take;  // rest < 32: one record per lane at most
+      int4 a0 = make_int4(0, 0, 0, 0), a1 = a0;
+      if (lane < rest) { a0 = sm.task[l][take + lane][0]; a1 = sm.task[l][take + lane][1]; }
+      __syncwarp();
+      if (lane < rest) { sm.task[l][lane][0] = a0; sm.task[l][lane][1] = a1; }
+      if (lane == 0) sm.nb[l + 1] = rest;
+      __syncwarp();
+    }
+  }
+
+  // One batch at level l: lanes with 'has' own the partial match in slot
+  // 'slot' (root lane for l = 0).  nbatch is informational.
+  template <int l>
+  __device__ __forceinline__ void level(bool has, int slot, int nbatch) {
+    (void)nbatch;
+    int m[N];
+    int e[KE];
+#pragma unroll
+    for (int q = 0; q < KE; q++) e[q] = 0;
+    Prev p = {0, 0, 0, 0, 0, 0};
+    int root = lane;
+    if (has) reconstruct<l>(slot, m, e, p, root);
+    else {
+#pragma unroll
+      for (int q = 0; q < N; q++) m[q] = -1;
+    }
+    if constexpr (l == 0) {
+      if (has) {
+        const int4 r = sm.root[slot];
+        const int e0 = r.w;
+        const int4 ed = __ldg(g.edges + e0);
+        p.eid = e0; p.t = ed.z; p.src = ed.x; p.dst = ed.y; p.pop = ed.w; p.pip = __ldg(g.inpos + e0);
       }
     }
+    int tl = sm.root[root].z;
 
-    // ----------------------------------------- issue this step's loads ----
-    int4 r0 = make_int4(0, 0, 0, 0), r1 = make_int4(0, 0, 0, 0);
-    int x0 = 0;
-    bool two = false;
-    {
-      const int4 *lst = out ? g.out_rec : g.in_rec;
-      if (mode == M_SCAN) {
-        r0 = __ldg(lst + pos);
-        two = WIDE && (level == L - 1) && (pos + 1 < end);
-        if (two) r1 = __ldg(lst + pos + 1);
-      } else if (mode == M_BS) {
-        const int mid = (pos + bhi) >> 1;
-        x0 = strict ? ld_t(lst + mid) : ld_eid(lst + mid);
-      } else if (mode == M_OPEN) {
-        r0 = __ldg(g.node_rng + n0);
-        if (n1 >= 0) r1 = __ldg(g.node_rng + n1);
-      } else if (mode == M_ROOT) {
-        r0 = __ldg(g.edges + n0);
-        x0 = __ldg(g.inpos + n0);
-      }
-    }
-
-    // ------------------------------------------------ process the step ----
-    bool emit = false;
-    int last_eid = 0;
-    if (mode == M_SCAN) {
-      ++pos;
-      if (r0.z > tl) {
-        pos = end;  // rest of the list is outside the window
-      } else if (structural_ok(r0.y)) {
-        if (level == L - 1) {
-          ++cnt;
-          if (ENUM) { emit = true; last_eid = r0.x; }
-        } else {
-          put(sp, level, pos);
-          put(se, level, end);
-          if (want < 0) put(m, nmc, r0.y);
-          if (ENUM) put(e, level + 1, r0.x);
-          const int psrc = out ? base : r0.y;
-          const int pdst = out ? r0.y : base;
-          const int pop = out ? pos - 1 : r0.w;
-          const int pip = out ? r0.w : pos - 1;
-          ++level;
-          prepare_open(level, r0.x, r0.z, psrc, pdst, pop, pip);
-        }
-      }
-      if (two && pos < end) {  // second record of a last-level step
-        ++pos;
-        if (r1.z > tl) pos = end;
-        else if (structural_ok(r1.y)) ++cnt;
-      }
-    } else if (mode == M_BS) {
-      const int mid = (pos + bhi) >> 1;
-      if (x0 > key) bhi = mid; else pos = mid + 1;
-      if (pos >= bhi) mode = M_SCAN;  // pos = first record after the previous edge
-    } else if (mode == M_OPEN) {
-      const int w = sel(info, level);
-      const int kind = plan_kind(w);
-      nmc = plan_nm(w);
+    // ------------------------------------------------------- open list ----
+    const int w = plan.info[l];
+    const int kind = plan_kind(w);
+    const int nmc = plan_nm(w);
+    int pos = 0, end = 0, want = -1, base = 0;
+    bool out = true;
+    int blo = 0, bhi = 0;
+    bool searching = false;
+    if (has) {
       const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
       int lo, hi, sc;
       if (kind == 2) {
-        if (r0.w - r0.z < r1.y - r1.x) { out = false; base = ib; want = ia; lo = r0.z; hi = r0.w; sc = sc0; }
-        else { out = true; base = ia; want = ib; lo = r1.x; hi = r1.y; sc = sc1; }
+        const int4 ri = __ldg(g.node_rng + ib);
+        const int4 ro = __ldg(g.node_rng + ia);
+        if (ri.w - ri.z < ro.y - ro.x) {
+          out = false; base = ib; want = ia; lo = ri.z; hi = ri.w;
+          sc = (p.dst == ib) ? p.pip + 1 : -1;
+        } else {
+          out = true; base = ia; want = ib; lo = ro.x; hi = ro.y;
+          sc = (p.src == ia) ? p.pop + 1 : -1;
+        }
       } else if (kind == 1) {
-        out = true; base = ia; want = -1; lo = r0.x; hi = r0.y; sc = sc1;
+        const int4 r = __ldg(g.node_rng + ia);
+        out = true; base = ia; lo = r.x; hi = r.y;
+        sc = (p.src == ia) ? p.pop + 1 : -1;
       } else {
-        out = false; base = ib; want = -1; lo = r0.z; hi = r0.w; sc = sc0;
+        const int4 r = __ldg(g.node_rng + ib);
+        out = false; base = ib; lo = r.z; hi = r.w;
+        sc = (p.dst == ib) ? p.pip + 1 : -1;
       }
-      iomask = (iomask & ~(1u << level)) | ((unsigned)out << level);
       end = hi;
-      if (!strict && sc >= 0) { pos = sc; mode = M_SCAN; }
-      else if (lo >= hi) { pos = hi; mode = M_SCAN; }
-      else { pos = lo; bhi = hi; mode = M_BS; }
-    } else if (mode == M_ROOT) {
-      if (r0.x == r0.y) {  // self-loops are not roots
-        mode = M_IDLE;
+      if (!strict && sc >= 0) {
+        pos = sc;
+      } else if (lo < hi) {
+        blo = lo; bhi = hi; searching = true;
       } else {
-        m[0] = r0.x;
-        m[1] = r0.y;
-        tl = r0.z + args.delta;
-        if (ENUM) e[0] = n0;
-        level = 0;
-        prepare_open(0, n0, r0.z, r0.x, r0.y, r0.w, x0);
+        pos = hi;
       }
     }
-    // exhausted ranges: pop to the deepest level with work left
-    while (mode == M_SCAN && pos >= end) {
-      if (level == 0) { mode = M_IDLE; level = -1; }
-      else { --level; pos = sel(sp, level); end = sel(se, level); restore(level); }
-    }
-
-    // ------------------------------------------- enumeration output ----
-    if (ENUM) {
-      const unsigned em = __ballot_sync(kFull, emit);
-      if (em) {
-        const int leader = __ffs(em) - 1;
-        unsigned long long b0 = 0;
-        if (lane == leader) b0 = atomicAdd(args.count, (unsigned long long)__popc(em));
-        b0 = __shfl_sync(kFull, b0, leader);
-        if (emit) {
-          const unsigned long long slot = b0 + (unsigned long long)__popc(em & lt_mask);
-          if (slot < (unsigned long long)args.cap) {
-            int *row = args.rows + slot * K;
-#pragma unroll
-            for (int q = 0; q < K - 1; q++) row[q] = __ldg(g.euid + e[q < KE ? q : 0]);
-            row[K - 1] = __ldg(g.euid + last_eid);
-          }
-          if (!args.exact_total && slot + 1 >= (unsigned long long)args.cap)
-            atomicExch(args.stop, 1);
+    // first record after the previous edge (by id; by time in strict mode)
+    {
+      const int key = strict ? p.t : p.eid;
+      while (__any_sync(kFull, searching)) {
+        if (searching) {
+          const int4 *lst = out ? g.out_rec : g.in_rec;
+          const int mid = (blo + bhi) >> 1;
+          const int v = strict ? ld_t(lst + mid) : ld_eid(lst + mid);
+          if (v > key) bhi = mid; else blo = mid + 1;
+          if (blo >= bhi) { searching = false; pos = blo; }
         }
       }
     }
 
-    // ---------------------------------------- tail: finish or steal ----
-    if (exhausted) {
-      const unsigned idle2 = __ballot_sync(kFull, mode == M_IDLE);
-      if (idle2 == kFull) break;
-      if (idle2 && args.steal_interval && (iter & (unsigned)(args.steal_interval - 1)) == 0) {
-        // shallowest level with a splittable remaining range, then widest
-        int sl = -1, sw = 0;
-        if (mode != M_IDLE) {
+    int steps = 0;
+    if constexpr (l == L - 1) {
+      // ------------------------------------------------ last level ----
+      while (true) {
+        const unsigned act = __ballot_sync(kFull, pos < end);
+        if (!act) break;
+        if (act != kFull && args.steal_interval && ((++steps) & (args.steal_interval - 1)) == 0)
+          rebalance(act, pos, end, want, out, base, slot, root, tl, m, e);
+        bool emit = false;
+        int last_eid = 0;
+        if (pos < end) {
+          const int4 *lst = out ? g.out_rec : g.in_rec;
+          int4 rr[WIDE];
 #pragma unroll
-          for (int l = 0; l < S; l++) {
-            if (sl < 0 && l < level) {
-              const int w = se[l] - sp[l];
-              if (w >= args.min_split) { sl = l; sw = w; }
-            }
-          }
-          if (sl < 0 && mode == M_SCAN && end - pos >= args.min_split) { sl = level; sw = end - pos; }
-        }
-        const unsigned skey = sl < 0 ? 0u : (((unsigned)(L - sl) << 24) | (unsigned)min(sw, 0xFFFFFF));
-        const unsigned kmax = __reduce_max_sync(kFull, skey);
-        if (kmax) {
-          const int donor = __ffs(__ballot_sync(kFull, skey == kmax)) - 1;
-          const int split_l = L - (int)(kmax >> 24);
-          int p0 = 0, p1 = 0;
-          if (lane == donor) {
-            const bool cur = (split_l == level);
-            p0 = cur ? pos : sel(sp, split_l);
-            p1 = cur ? end : sel(se, split_l);
-            const bool o = (iomask >> split_l) & 1u;
-            p1 = first_t_after(o ? g.out_rec : g.in_rec, p0, p1, tl);  // window end
-            if (cur) end = p1; else put(se, split_l, p1);
-          }
-          p0 = __shfl_sync(kFull, p0, donor);
-          p1 = __shfl_sync(kFull, p1, donor);
-          const int w = p1 - p0;
-          const int nthief = min(__popc(idle2), w - 1);
-          if (nthief > 0) {
-            const int parts = nthief + 1;
-            const int rank = __popc(idle2 & lt_mask);
-            const bool thief = (mode == M_IDLE) && rank < nthief;
+          for (int q = 0; q < WIDE; q++)
+            if (q == 0 || pos + q < end) rr[q] = __ldg(lst + pos + q);
 #pragma unroll
-            for (int q = 0; q < N; q++) {
-              const int x = __shfl_sync(kFull, m[q], donor);
-              if (thief) m[q] = x;
-            }
-            if (ENUM) {
-#pragma unroll
-              for (int q = 0; q < KE; q++) {
-                const int x = __shfl_sync(kFull, e[q], donor);
-                if (thief) e[q] = x;
+          for (int q = 0; q < WIDE; q++) {
+            if (pos < end) {
+              ++pos;
+              if (rr[q].z > tl) {
+                pos = end;
+              } else if (structural_ok(rr[q].y, want, nmc, m)) {
+                ++cnt;
+                if (ENUM) { emit = true; last_eid = rr[q].x; }
               }
             }
-            const int dtl = __shfl_sync(kFull, tl, donor);
-            const unsigned dio = __shfl_sync(kFull, iomask, donor);
-            if (thief) {
-              tl = dtl;
-              iomask = dio;
-              level = split_l;
-              mode = M_SCAN;
-              pos = p0 + (int)((long long)w * (rank + 1) / parts);
-              end = p0 + (int)((long long)w * (rank + 2) / parts);
-#pragma unroll
-              for (int q = 0; q < S; q++) { sp[q] = 0; se[q] = 0; }
-              restore(split_l);
-            }
-            if (lane == donor) {
-              const int ne = p0 + (int)((long long)w / parts);
-              if (split_l == level) end = ne; else put(se, split_l, ne);
-            }
-          } else if (lane == donor) {
-            // nothing to split after trimming: drop an exhausted range
-            while (mode == M_SCAN && pos >= end) {
-              if (level == 0) { mode = M_IDLE; level = -1; }
-              else { --level; pos = sel(sp, level); end = sel(se, level); restore(level); }
-            }
           }
+        }
+        if constexpr (ENUM) emit_row(emit, e, last_eid);
+      }
+    } else {
+      // --------------------------------- scan, queue children, descend ----
+      // The level before the last one counts a closing last edge inline by
+      // range arithmetic on the pair index (count mode only).
+      const bool inline_last = (l == L - 2) && !ENUM && args.inline_last;
+      const int wl = plan.info[L - 1];
+      const int la = plan_a(wl), lb = plan_b(wl);
+      int ca = -1, cb = -1, ctl = 0, cs = 0, cub = 0, ckey = 0;  // this lane's pair cursor
+      while (true) {
+        const unsigned act = __ballot_sync(kFull, pos < end);
+        if (!inline_last) {
+          const int nb = sm.nb[l + 1];
+          if (nb >= 32 || (!act && nb > 0)) {
+            // park this level's state in shared memory while the warp descends,
+            // so none of it stays live in registers across the nested batch
+            sm.save[l][lane][0] = make_int4(pos, end, want, base);
+            sm.save[l][lane][1] = make_int4(slot, root, tl, (steps << 1) | (out ? 1 : 0));
+            __syncwarp();
+            descend<l>();
+            const int4 s0 = sm.save[l][lane][0], s1 = sm.save[l][lane][1];
+            pos = s0.x; end = s0.y; want = s0.z; base = s0.w;
+            slot = s1.x; root = s1.y; tl = s1.z; out = (s1.w & 1) != 0; steps = s1.w >> 1;
+            Prev dummy;
+            int rr;
+            if (pos < end) reconstruct<l>(slot, m, e, dummy, rr);
+            continue;
+          }
+        }
+        if (!act) break;
+        if (act != kFull && args.steal_interval && ((++steps) & (args.steal_interval - 1)) == 0)
+          rebalance(act, pos, end, want, out, base, slot, root, tl, m, e);
+        bool push = false;
+        int4 rc = make_int4(0, 0, 0, 0);
+        if (pos < end) {
+          const int4 *lst = out ? g.out_rec : g.in_rec;
+          rc = __ldg(lst + pos);
+          ++pos;
+          if (rc.z > tl) pos = end;
+          else push = structural_ok(rc.y, want, nmc, m);
+        }
+        if (inline_last) {
+          if (push) {
+            // the last edge joins two nodes mapped before this level, so its
+            // pair run is fixed for the task: keep a cursor into it that only
+            // moves forward as this lane's candidates advance
+            const int ia = sel(m, la), ib = sel(m, lb);
+            const int key = strict ? rc.z : rc.x;
+            if (ia != ca || ib != cb || tl != ctl || key < ckey) {
+              const int2 f = pair_find(g, ia, ib);
+              ca = ia; cb = ib; ctl = tl;
+              cub = pair_first_t_after(g, f.x, f.x + f.y, tl);
+              cs = pair_first_key_after(g, f.x, cub, key, strict != 0);
+            } else {
+              // a few steps forward; fall back to a search for long jumps
+              int steps_left = 4;
+              while (cs < cub && steps_left-- > 0 &&
+                     (strict ? __ldg(&g.pair_rec[cs].y) : __ldg(&g.pair_rec[cs].x)) <= key) ++cs;
+              if (steps_left < 0) cs = pair_first_key_after(g, cs, cub, key, strict != 0);
+            }
+            ckey = key;
+            cnt += (unsigned long long)(cub - cs);
+          }
+        } else {
+          push_children<l>(push, slot, rc, out, base, pos - 1, root);
         }
       }
     }
   }
 
-  if (!ENUM) {
+  // Idle lanes take equal slices of the widest remaining range at this level.
+  template <int NN, int EE>
+  __device__ __forceinline__ void rebalance(unsigned act, int &pos, int &end, int &want, bool &out,
+                                            int &base, int &slot, int &root, int &tl, int (&m)[NN],
+                                            int (&e)[EE]) {
+    const int width = end - pos;
+    const unsigned wmax = __reduce_max_sync(kFull, (unsigned)(width > 0 ? width : 0));
+    if ((int)wmax < args.min_split) return;
+    const int donor = __ffs(__ballot_sync(kFull, (unsigned)width == wmax)) - 1;
+    const unsigned idle = ~act;
+    const int nthief = min(__popc(idle), (int)wmax - 1);
+    if (nthief <= 0) return;
+    const int parts = nthief + 1;
+    const int rank = __popc(idle & lt);
+    const bool thief = ((idle >> lane) & 1u) && rank < nthief;
+    const int p0 = __shfl_sync(kFull, pos, donor);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(kFull, cnt, o);
-    if (lane == 0 && cnt) atomicAdd(args.count, cnt);
+    for (int q = 0; q < NN; q++) {
+      const int x = __shfl_sync(kFull, m[q], donor);
+      if (thief) m[q] = x;
+    }
+    if (ENUM) {
+#pragma unroll
+      for (int q = 0; q < EE; q++) {
+        const int x = __shfl_sync(kFull, e[q], donor);
+        if (thief) e[q] = x;
+      }
+    }
+    const int d_want = __shfl_sync(kFull, want, donor);
+    const int d_out = __shfl_sync(kFull, (int)out, donor);
+    const int d_base = __shfl_sync(kFull, base, donor);
+    const int d_slot = __shfl_sync(kFull, slot, donor);
+    const int d_root = __shfl_sync(kFull, root, donor);
+    const int d_tl = __shfl_sync(kFull, tl, donor);
+    const int w = (int)wmax;
+    if (thief) {
+      want = d_want; out = d_out != 0; base = d_base; slot = d_slot; root = d_root; tl = d_tl;
+      pos = p0 + (int)((long long)w * (rank + 1) / parts);
+      end = p0 + (int)((long long)w * (rank + 2) / parts);
+    }
+    if (lane == donor) end = p0 + (int)((long long)w / parts);
+  }
+
+  __device__ __forceinline__ void emit_row(bool emit, const int (&e)[KE], int last_eid) {
+    const unsigned em = __ballot_sync(kFull, emit);
+    if (!em) return;
+    const int leader = __ffs(em) - 1;
+    unsigned long long b0 = 0;
+    if (lane == leader) b0 = atomicAdd(args.count, (unsigned long long)__popc(em));
+    b0 = __shfl_sync(kFull, b0, leader);
+    if (emit) {
+      const unsigned long long s = b0 + (unsigned long long)__popc(em & lt);
+      if (s < (unsigned long long)args.cap) {
+        int *row = args.rows + s * K;
+#pragma unroll
+        for (int q = 0; q < K - 1; q++) row[q] = __ldg(g.euid + e[q < KE ? q : 0]);
+        row[K - 1] = __ldg(g.euid + last_eid);
+      }
+      if (!args.exact_total && s + 1 >= (unsigned long long)args.cap) atomicExch(args.stop, 1);
+    }
+  }
+};
+
+template <int K, bool ENUM>
+__global__ void __launch_bounds__(kBlock)
+search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
+  extern __shared__ int4 dyn_smem[];
+  WarpSmem<K> *smem = reinterpret_cast<WarpSmem<K> *>(dyn_smem);
+  const int lane = threadIdx.x & 31;
+  WarpSmem<K> &sm = smem[threadIdx.x >> 5];
+  if (lane < K) sm.nb[lane] = 0;
+  __syncwarp();
+  Searcher<K, ENUM> S(g, plan, args, sm, lane);
+  const int batch = 32;
+  while (true) {
+    int b0 = 0;
+    if (lane == 0) {
+      if (ENUM && *(volatile int *)args.stop) b0 = args.root_end;
+      else b0 = atomicAdd(args.cursor, batch);
+    }
+    b0 = __shfl_sync(kFull, b0, 0);
+    if (b0 >= args.root_end) break;
+    const int r = b0 + lane;
+    bool has = false;
+    if (r < args.root_end) {
+      const int4 ed = __ldg(g.edges + r);
+      if (ed.x != ed.y) {  // self-loops are not roots
+        sm.root[lane] = make_int4(ed.x, ed.y, ed.z + args.delta, r);
+        has = true;
+      }
+    }
+    __syncwarp();
+    if (K == 2 && !ENUM && args.inline_last) {
+      // the only searched edge closes on the root's endpoints
+      if (has) {
+        const int4 rt = sm.root[lane];
+        const int w = plan.info[0];
+        const int ia = plan_a(w) == 0 ? rt.x : rt.y, ib = plan_b(w) == 0 ? rt.x : rt.y;
+        const int2 f = pair_find(g, ia, ib);
+        const int key = args.strict_ts ? rt.z - args.delta : rt.w;
+        S.cnt += (unsigned long long)pair_window(g, f.x, f.y, key, rt.z, args.strict_ts != 0);
+      }
+    } else {
+      S.template level<0>(has, lane, 32);
+    }
+    __syncwarp();
+  }
+  if (!ENUM) {
+    unsigned long long c = S.cnt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+    if (lane == 0 && c) atomicAdd(args.count, c);
   }
 }
 
 template <int K, bool ENUM>
-int launch_k(const GraphView &g, const MotifPlan &plan, const SearchArgs &args, int grid,
-             int block, cudaStream_t s) {
-  search_kernel<K, ENUM><<<grid, block, 0, s>>>(g, plan, args);
+int setup_k() {
+  static bool done = false;  // per process; the attribute is per function
+  if (!done) {
+    cudaError_t e = cudaFuncSetAttribute(search_kernel<K, ENUM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kWarps * sizeof(WarpSmem<K>)));
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    done = true;
+  }
+  return 0;
+}
+
+template <int K, bool ENUM>
+int launch_k(const GraphView &g, const MotifPlan &plan, const SearchArgs &args, int grid, int block,
+             cudaStream_t s) {
+  (void)block;
+  int rc = setup_k<K, ENUM>();
+  if (rc) return rc;
+  search_kernel<K, ENUM><<<grid, kBlock, kWarps * sizeof(WarpSmem<K>), s>>>(g, plan, args);
   return 0;
 }
 
 template <int K, bool ENUM>
 int occ_k(int block, int *bps) {
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, search_kernel<K, ENUM>, block, 0);
+  (void)block;
+  int rc = setup_k<K, ENUM>();
+  if (rc) return rc;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, search_kernel<K, ENUM>, kBlock,
+                                                                kWarps * sizeof(WarpSmem<K>));
   return e == cudaSuccess ? 0 : cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
 }
 
@@ -436,8 +595,8 @@ int occ_k(int block, int *bps) {
     default: return fail(EVX_ERR_INVALID, "motif edge count out of range");          \
   }
 
-int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &args, int grid,
-                  int block, cudaStream_t stream) {
+int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &args, int grid, int block,
+                  cudaStream_t stream) {
   const int k = plan.k;
   const bool enumerate = args.enumerate != 0;
   EVX_K_DISPATCH(launch_k, g, plan, args, grid, block, stream)
@@ -446,5 +605,7 @@ int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &a
 int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm) {
   EVX_K_DISPATCH(occ_k, block, blocks_per_sm)
 }
+
+int search_block_size() { return kBlock; }
 
 }  // namespace evx

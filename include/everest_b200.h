@@ -43,6 +43,7 @@ extern "C" {
 #define EVX_FLAG_STRICT_TS 1u    /* additionally require t(e_j) > t(e_{j-1}) */
 #define EVX_FLAG_EXACT_TOTAL 2u  /* enumerate: keep counting past the cap */
 #define EVX_FLAG_NO_STEAL 4u     /* disable intra-warp work stealing */
+#define EVX_FLAG_NO_PAIR_INDEX 8u /* count the last edge by scanning, not range arithmetic */
 
 typedef struct evx_graph evx_graph;   /* a graph resident on one device */
 typedef struct evx_worker evx_worker; /* per-device search worker */
