@@ -33,8 +33,9 @@ EXPORTS = [
     "evx_graph_from_device", "evx_graph_free", "evx_graph_info", "evx_worker_create",
     "evx_worker_destroy", "evx_worker_stream", "evx_worker_take", "evx_worker_run",
     "evx_worker_launch", "evx_worker_result", "evx_worker_enum_rows", "evx_worker_set_tuning",
-    "evx_worker_last_stats", "evx_host_register", "evx_host_unregister",
+    "evx_worker_last_stats", "evx_host_register", "evx_host_unregister", "evx_count_static",
 ]
+STATIC_MAX_QUERIES = 256
 
 
 class EvxError(RuntimeError):
@@ -70,6 +71,8 @@ def lib():
             "evx_free": ([_P], None),
             "evx_host_register": ([_P, _I64], _I),
             "evx_host_unregister": ([_P], _I),
+            "evx_count_static": ([_P, _I, _PI, _PI, _PI, _PI, _I64, _I64, ctypes.c_uint, _P,
+                                  _PU64], _I),
             "evx_graph_upload": ([_I, _I64, _I64, _P, _P, _P, _P, _P, _P, _P,
                                   ctypes.POINTER(_P)], _I),
             "evx_graph_from_device": ([_I, _I64, _I64, _P, _P, _P, _P, _P, _P, _P,
@@ -285,6 +288,24 @@ class DeviceGraph:
             self.free()
         except Exception:
             pass
+
+
+def count_static(graph: "DeviceGraph", queries, beg: int = 0, end: int = -1, flags: int = 0,
+                 stream: Optional[int] = None):
+    """Count queries [(mu, mv, delta), ...] through the allocation-free entry
+    point (for callers that cannot allocate device memory at query time)."""
+    nq = len(queries)
+    ks = [len(q[0]) for q in queries]
+    mu = [x for q in queries for x in q[0]]
+    mv = [x for q in queries for x in q[1]]
+    a_k = (ctypes.c_int * max(nq, 1))(*ks)
+    a_mu = (ctypes.c_int * max(len(mu), 1))(*mu)
+    a_mv = (ctypes.c_int * max(len(mv), 1))(*mv)
+    a_d = (ctypes.c_int * max(nq, 1))(*[int(q[2]) for q in queries])
+    out = (ctypes.c_uint64 * max(nq, 1))()
+    check(lib().evx_count_static(graph.handle, nq, a_k, a_mu, a_mv, a_d, int(beg), int(end),
+                                 int(flags), ctypes.c_void_p(stream) if stream else None, out))
+    return [int(out[i]) for i in range(nq)]
 
 
 # --------------------------------------------------------------- worker --

@@ -30,7 +30,7 @@ int graph_t_range(DeviceGraph &g, int *scratch_d, cudaStream_t s);
 
 // Decode a relabeled motif into the per-level plan (HostMotifData rules,
 // src/core/cpu/data.cc:416-446).
-static int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
+int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
   if (k < 2 || k > EVX_MAX_MOTIF_EDGES)
     return fail(EVX_ERR_INVALID, "motif must have 2.." + std::to_string(EVX_MAX_MOTIF_EDGES) + " edges");
   if (mu[0] != 0 || mv[0] != 1)
@@ -67,10 +67,6 @@ static int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
 }  // namespace evx
 
 using namespace evx;
-
-struct evx_graph {
-  DeviceGraph g;
-};
 
 struct evx_worker {
   int device = 0;

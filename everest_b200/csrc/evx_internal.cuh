@@ -111,6 +111,9 @@ struct DeviceGraph {
   }
 };
 
+// Decode relabeled motif edges into the per-level plan (evx_capi.cu).
+int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan);
+
 // Error plumbing (thread-local message).
 void set_error(const std::string &msg);
 int fail(int code, const std::string &msg);
@@ -137,3 +140,8 @@ int pack_graph(DeviceGraph &g, const int *eg_d, const int *out_v_d, const int *i
                const int *out_r_d, const int *in_r_d, const int *euid_d, cudaStream_t s);
 
 }  // namespace evx
+
+// The opaque graph handle of the C ABI.
+struct evx_graph {
+  evx::DeviceGraph g;
+};

@@ -162,6 +162,24 @@ EVX_API int evx_worker_set_tuning(evx_worker *w, int block, int blocks_per_sm,
  * and device milliseconds measured with CUDA events around them. */
 EVX_API int evx_worker_last_stats(evx_worker *w, int *kernel_launches, float *device_ms);
 
+/* ------------------------------------------------- allocation-free count --
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * at query time (device memory fully reserved by another allocator, or a
+ * device with no free memory left): runs nq count queries (1 <=
+ * nq <= EVX_STATIC_MAX_QUERIES) on a resident graph and writes the counts to
+ * counts[nq] (host memory), with no cudaMalloc / cudaFree / allocating call.
+ * Its scratch is a file-scope device array of EVX_STATIC_MAX_QUERIES slots
+ * (4 KB per device, held until the process exits).  Query q is motif edges
+ * mu/mv[off_q .. off_q + k[q]) with off_q = k[0] + ... + k[q-1], window
+ * delta[q]; roots are [beg, end) (end < 0: E - k + 1).  The first call on a
+ * device looks up the array's device address, so it must come before any
+ * stream capture.  All calls share the array: calls whose GPU work overlaps
+ * race, so serialise them.  Rejects nq > EVX_STATIC_MAX_QUERIES. */
+#define EVX_STATIC_MAX_QUERIES 256
+EVX_API int evx_count_static(const evx_graph *g, int nq, const int *k, const int *mu,
+                             const int *mv, const int *delta, int64_t beg, int64_t end,
+                             unsigned flags, void *stream, uint64_t *counts);
+
 #ifdef __cplusplus
 }
 #endif
