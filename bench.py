@@ -155,6 +155,17 @@ def dist_setup(gpus):
     return world, rank, local, dist
 
 
+def max_over_ranks(value: float, dist, device=None) -> float:
+    """Max of a per-rank value over all ranks (identity on one rank)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64,
+                     device=device if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # --------------------------------------------------------- CPU reference --
 
 def cpu_reference(wname, root_frac, threads):
@@ -268,11 +279,7 @@ def run_gpu_arm(args):
             kern_ms.append(kms)
             launches += nl
     barrier()
-    total_ms = sum(step_ms)
-    if dist is not None:
-        tt = torch.tensor([total_ms], device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = max_over_ranks(sum(step_ms), dist, f"cuda:{dev}")
     matches = sum(counts)
     ms_per_step = total_ms / args.steps
     value = world * matches / (ms_per_step / 1e3)
@@ -302,11 +309,7 @@ def run_gpu_arm(args):
         ms, cs = e2e_step()
         e_ms.append(ms)
     barrier()
-    e_total = sum(e_ms)
-    if dist is not None:
-        tt = torch.tensor([e_total], device=f"cuda:{dev}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e_total = float(tt.item())
+    e_total = max_over_ranks(sum(e_ms), dist, f"cuda:{dev}")
     e2e_val = world * sum(cs) / (e_total / args.steps / 1e3)
     h2d = host.total_bytes + sum(8 * len(q["mu"]) for q in qs)
     d2h = 8 * len(qs)

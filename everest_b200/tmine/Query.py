@@ -1,0 +1,123 @@
+"""YAML query model (the reference's system/tmine/Query.py:6-37,311-338).
+
+    pattern: M3.txt            # motif file (u v t lines)
+    graph: wiki-talk.txt       # temporal edge list (u v t lines)
+    constraints:
+      delta: 86400
+    options:
+      gpu: 1
+      enumerate: 1000          # optional: enumerate up to this many rows
+      warpCentric: True        # accepted; the kernels are always warp-centric
+      warpBalancing: True      # False disables work stealing
+      tailExpansion: True      # False disables range-arithmetic tail counting
+
+Label, fine-grained temporal, anti-edge and filter constraints are not on
+this path and are rejected with NotImplementedError.
+"""
+import os
+
+import yaml
+
+from . import locations
+
+DEFAULT_OPTIONS = {"gpu": 1, "warpCentric": True, "warpBalancing": True, "tailExpansion": True}
+UNSUPPORTED = ("temporal", "antiEdge", "filter")
+
+
+class Options:
+    def __init__(self, opts=None):
+        self.opts = dict(DEFAULT_OPTIONS)
+        if opts:
+            self.opts.update(opts)
+        if self.multigpu():
+            self.opts["multigpu"] = True
+
+    def gpu(self) -> int:
+        return int(self.opts["gpu"])
+
+    def multigpu(self) -> bool:
+        return int(self.opts["gpu"]) > 1
+
+    def enumerate(self) -> bool:
+        return "enumerate" in self.opts
+
+    def enumNum(self) -> int:
+        return int(self.opts["enumerate"])
+
+    def flags(self) -> int:
+        """EVX_FLAG_* bits the options select."""
+        f = 0
+        if not self.opts.get("warpBalancing", True):
+            f |= 4
+        if not self.opts.get("tailExpansion", True):
+            f |= 8
+        if self.opts.get("strictTimestamps", False):
+            f |= 1
+        return f
+
+    def __repr__(self):
+        return f"Options:\n {self.opts}"
+
+
+class Constraints:
+    def __init__(self, cons):
+        self.cons = dict(cons or {})
+        bad = [k for k in self.cons if k in UNSUPPORTED or k.startswith("node") or k.startswith("edge")]
+        if bad:
+            raise NotImplementedError(
+                f"constraints {bad} (labels, fine-grained temporal windows, anti-edges, filters) "
+                "are not supported by this miner; only 'delta' is")
+        if "delta" not in self.cons:
+            raise ValueError("query constraints need 'delta'")
+
+    def isDelta(self) -> bool:
+        return "delta" in self.cons
+
+    def delta(self) -> int:
+        return int(self.cons["delta"])
+
+    def genConsTemplates(self):
+        """No code generation on this path (kept for call compatibility)."""
+        return None
+
+    def __repr__(self):
+        return f"Constraints:\n {self.cons}"
+
+
+def _resolve(name: str, root: str, base_dir: str) -> str:
+    if os.path.isabs(name) and os.path.exists(name):
+        return name
+    for cand in (os.path.join(root, name), os.path.join(base_dir, name)):
+        if os.path.exists(cand):
+            return cand
+    return os.path.join(root, name)
+
+
+class Query:
+    def __init__(self, pathToQuery: str):
+        with open(pathToQuery) as f:
+            self.queryFile = yaml.safe_load(f)
+        self.name = pathToQuery
+        base = os.path.dirname(os.path.abspath(pathToQuery))
+        for key in ("pattern", "graph", "constraints"):
+            if key not in self.queryFile:
+                raise ValueError(f"query {pathToQuery} has no '{key}'")
+        self.cons = Constraints(self.queryFile["constraints"])
+        self.opts = Options(self.queryFile.get("options") or {})
+        self.queryFile["pattern"] = _resolve(str(self.queryFile["pattern"]), locations.inputMotifsRoot(), base)
+        self.queryFile["graph"] = _resolve(str(self.queryFile["graph"]), locations.inputGraphRoot(), base)
+
+    def pattern(self) -> str:
+        return self.queryFile["pattern"]
+
+    def graph(self) -> str:
+        return self.queryFile["graph"]
+
+    def constraints(self) -> Constraints:
+        return self.cons
+
+    def options(self) -> Options:
+        return self.opts
+
+    def __repr__(self):
+        return f"Query {self.name}:\n {self.queryFile}"
