@@ -34,6 +34,8 @@ EXPORTS = [
     "evx_worker_destroy", "evx_worker_stream", "evx_worker_take", "evx_worker_run",
     "evx_worker_launch", "evx_worker_result", "evx_worker_enum_rows", "evx_worker_set_tuning",
     "evx_worker_last_stats", "evx_host_register", "evx_host_unregister", "evx_count_static",
+    "evx_batch_create", "evx_batch_destroy", "evx_batch_add", "evx_batch_clear", "evx_batch_launch",
+    "evx_batch_result", "evx_batch_run", "evx_batch_set_tuning", "evx_batch_last_stats",
 ]
 STATIC_MAX_QUERIES = 256
 
@@ -89,7 +91,7 @@ def lib():
             "evx_worker_enum_rows": ([_P, _I64, _P, _PI64], _I),
             "evx_worker_set_tuning": ([_P, _I, _I, _I, _I, _I], _I),
             "evx_worker_last_stats": ([_P, _PI, ctypes.POINTER(ctypes.c_float)], _I),
-            "evx_batch_create": ([_I, _P, ctypes.POINTER(_P)], _I),
+            "evx_batch_create": ([_I, _I, _P, ctypes.POINTER(_P)], _I),
             "evx_batch_destroy": ([_P], _I),
             "evx_batch_add": ([_P, _P, _I, _PI, _PI, _I, _I64, _I64, ctypes.c_uint, _PI], _I),
             "evx_batch_clear": ([_P], _I),
@@ -372,6 +374,64 @@ class Worker:
     def close(self):
         if getattr(self, "_h", None):
             lib().evx_worker_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# -------------------------------------------------------------- batches --
+
+class Batch:
+    """Many count queries on one resident graph in one persistent launch."""
+
+    def __init__(self, device: int = 0, max_queries: int = 1024, stream: Optional[int] = None):
+        h = ctypes.c_void_p()
+        check(lib().evx_batch_create(int(device), int(max_queries),
+                                     ctypes.c_void_p(stream) if stream else None, ctypes.byref(h)))
+        self._h = h
+        self.n = 0
+
+    def set_tuning(self, tile_roots=256, blocks_per_sm=0, steal_interval=16, min_split=2, use_graph=True):
+        check(lib().evx_batch_set_tuning(self._h, tile_roots, blocks_per_sm, steal_interval, min_split,
+                                         1 if use_graph else 0, 0))
+
+    def add(self, graph: DeviceGraph, mu, mv, delta, beg=0, end=-1, flags=0) -> int:
+        k = len(mu)
+        idx = ctypes.c_int(0)
+        check(lib().evx_batch_add(self._h, graph.handle, k, (ctypes.c_int * k)(*mu), (ctypes.c_int * k)(*mv),
+                                  int(delta), int(beg), int(end), int(flags), ctypes.byref(idx)))
+        self.n += 1
+        return idx.value
+
+    def clear(self):
+        check(lib().evx_batch_clear(self._h))
+        self.n = 0
+
+    def launch(self):
+        check(lib().evx_batch_launch(self._h))
+
+    def result(self):
+        out = (ctypes.c_uint64 * max(self.n, 1))()
+        check(lib().evx_batch_result(self._h, out, self.n))
+        return [int(out[i]) for i in range(self.n)]
+
+    def run(self):
+        self.launch()
+        return self.result()
+
+    def last_stats(self):
+        n = ctypes.c_int()
+        ms = ctypes.c_float()
+        check(lib().evx_batch_last_stats(self._h, ctypes.byref(n), ctypes.byref(ms)))
+        return {"kernel_launches": n.value, "device_ms": ms.value}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().evx_batch_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -64,6 +64,25 @@ int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
   return EVX_OK;
 }
 
+// Range arithmetic on the pair index replaces the last level's scan (count
+// mode) when the last edge closes on two nodes mapped before the
+// second-to-last edge (its pair is fixed per partial match: kQInlineLast),
+// or repeats the second-to-last edge's endpoints (its pair run is the one
+// the matched edge sits in: kQSamePair).
+int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
+  const int k = plan.k;
+  if (enumerate || (flags & EVX_FLAG_NO_PAIR_INDEX) || k < 2) return 0;
+  const int wl = plan.info[k - 2];
+  if (plan_kind(wl) != 2) return 0;
+  const int nm_prev = (k >= 3) ? plan_nm(plan.info[k - 3]) : 2;
+  if (plan_a(wl) < nm_prev && plan_b(wl) < nm_prev) return kQInlineLast;
+  if (k >= 3) {
+    const int wp = plan.info[k - 3];
+    if (plan_a(wp) == plan_a(wl) && plan_b(wp) == plan_b(wl)) return kQSamePair;
+  }
+  return 0;
+}
+
 }  // namespace evx
 
 using namespace evx;
@@ -252,6 +271,7 @@ int evx_graph_free(evx_graph *h) {
   cudaSetDevice(g.device);
   cudaFree(g.edges); cudaFree(g.inpos); cudaFree(g.euid); cudaFree(g.out_rec);
   cudaFree(g.in_rec); cudaFree(g.node_rng); cudaFree(g.pair_tab); cudaFree(g.pair_rec);
+  cudaFree(g.pair_loc);
   delete h;
   return EVX_OK;
 }
@@ -381,16 +401,7 @@ int evx_worker_take(evx_worker *w, const evx_graph *gh, int k, const int *mu, co
   a.steal_interval = (flags & EVX_FLAG_NO_STEAL) ? 0 : w->steal_interval;
   a.min_split = w->min_split;
   a.enumerate = enum_cap > 0 ? 1 : 0;
-  {
-    // Range arithmetic on the pair index for the last edge when it closes
-    // on two nodes mapped before the second-to-last edge (its pair is then
-    // fixed per partial match); for k == 2 the root maps both.
-    const int wl = plan.info[k - 2];
-    const int nm_prev = (k >= 3) ? plan_nm(plan.info[k - 3]) : 2;
-    const bool fixed_pair = plan_a(wl) < nm_prev && plan_b(wl) < nm_prev;
-    a.inline_last = (enum_cap <= 0 && !(flags & EVX_FLAG_NO_PAIR_INDEX) && plan_kind(wl) == 2 &&
-                     fixed_pair) ? 1 : 0;
-  }
+  a.tail_flags = tail_mode(plan, flags, enum_cap > 0);
   a.exact_total = (flags & EVX_FLAG_EXACT_TOTAL) ? 1 : 0;
   a.cap = enum_cap;
   a.rows = w->rows_d;
@@ -406,7 +417,7 @@ int evx_worker_take(evx_worker *w, const evx_graph *gh, int k, const int *mu, co
 namespace evx {
 __global__ void reset_state_kernel(unsigned long long *count, int *cursor, int *stop, int beg) {
   *count = 0ull;
-  *cursor = beg;
+  *cursor = beg;  // the search's work queue: next unclaimed root tile
   *stop = 0;
 }
 }  // namespace evx
@@ -426,7 +437,7 @@ int evx_worker_launch(evx_worker *w) {
   const int64_t warps = (int64_t)grid * (w->block / 32);
   if ((int64_t)a.root_end + warps * (int64_t)a.roots_per_fetch >= (int64_t)INT_MAX)
     return fail(EVX_ERR_OVERFLOW, "root cursor would overflow int32");
-  reset_state_kernel<<<1, 1, 0, w->stream>>>(a.count, a.cursor, a.stop, a.root_beg);
+  reset_state_kernel<<<1, 1, 0, w->stream>>>(a.count, a.cursor, a.stop, 0);
   EVX_CUDA(cudaGetLastError());
   EVX_CUDA(cudaEventRecord(w->ev0, w->stream));
   int launches = 1;

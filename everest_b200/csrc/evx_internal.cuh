@@ -29,6 +29,7 @@ struct GraphView {
   const int4 *node_rng;
   const int4 *pair_tab;
   const int2 *pair_rec;
+  const int2 *pair_loc;       // [e] = {position of e in pair_rec, end of its run}
   unsigned long long pair_mask;
   int pair_max_probe;
   int num_edges;
@@ -66,6 +67,40 @@ __host__ __device__ inline int plan_a(int w) { return (w >> 4) & 15; }
 __host__ __device__ inline int plan_b(int w) { return (w >> 8) & 15; }
 __host__ __device__ inline int plan_nm(int w) { return (w >> 12) & 15; }
 
+// One query of a search launch (a table of these drives the batched kernel).
+constexpr int kQStrict = 1;      // t(e_j) > t(e_{j-1}) as well
+constexpr int kQInlineLast = 2;  // closing last edge counted on the pair index
+constexpr int kQSamePair = 4;    // last edge repeats the previous edge's endpoints
+struct QueryDesc {
+  MotifPlan plan;
+  int root_beg, root_end;  // root edge ids [beg, end)
+  int delta;
+  int flags;               // kQ* bits
+  int steal_interval;      // steps between rebalances (power of two), 0 = never
+  int min_split;           // smallest range worth splitting
+  int tile_beg;            // first work-queue tile of this query
+  int pad;
+};
+
+// Enumeration outputs (single-query enumerate launches only).
+struct EnumArgs {
+  int *rows;                  // [cap * k] original line ids
+  long long cap;
+  int exact_total;            // keep counting past the cap
+  int *stop;                  // set when the cap is reached: stop claiming roots
+  unsigned long long *count;  // slot counter (= reported count)
+};
+
+// A search launch: nq queries sharing one work queue of root tiles.
+struct LaunchArgs {
+  const QueryDesc *table;     // device table (nq > 1); ignored when nq == 1
+  int nq;
+  int total_tiles;
+  int tile_roots;             // roots per tile (multiple of 32)
+  int *cursor;                // next unclaimed tile
+  unsigned long long *counts; // [nq] per-query counts
+};
+
 // Search job arguments (one query).
 struct SearchArgs {
   int root_beg, root_end;     // root edge ids [beg, end)
@@ -75,7 +110,7 @@ struct SearchArgs {
   int steal_interval;         // iterations between steal checks (power of 2), 0 = off
   int min_split;              // smallest range width worth splitting
   int enumerate;              // 1: write rows
-  int inline_last;            // count a closing last edge by range arithmetic on the pair index
+  int tail_flags;             // kQInlineLast / kQSamePair: how the last edge is counted
   int exact_total;            // enumerate: keep counting past the cap
   long long cap;              // enumeration rows capacity
   int *rows;                  // [cap * k] original line ids
@@ -97,6 +132,7 @@ struct DeviceGraph {
   int4 *node_rng = nullptr;
   int4 *pair_tab = nullptr;
   int2 *pair_rec = nullptr;
+  int2 *pair_loc = nullptr;
   unsigned long long pair_mask = 0;
   int pair_max_probe = 0;
   int64_t bytes = 0;
@@ -104,7 +140,7 @@ struct DeviceGraph {
     GraphView g;
     g.edges = edges; g.inpos = inpos; g.euid = euid; g.out_rec = out_rec; g.in_rec = in_rec;
     g.node_rng = node_rng;
-    g.pair_tab = pair_tab; g.pair_rec = pair_rec; g.pair_mask = pair_mask;
+    g.pair_tab = pair_tab; g.pair_rec = pair_rec; g.pair_loc = pair_loc; g.pair_mask = pair_mask;
     g.pair_max_probe = pair_max_probe;
     g.num_edges = (int)num_edges; g.num_vertices = (int)num_vertices;
     return g;
@@ -113,6 +149,8 @@ struct DeviceGraph {
 
 // Decode relabeled motif edges into the per-level plan (evx_capi.cu).
 int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan);
+// How a count query counts its last edge (kQInlineLast, kQSamePair or 0).
+int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate);
 
 // Error plumbing (thread-local message).
 void set_error(const std::string &msg);
@@ -128,6 +166,11 @@ int cuda_fail(cudaError_t e, const char *what);
 // Launch the search for one query (defined in evx_search.cu).
 int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &args,
                   int grid, int block, cudaStream_t stream);
+// Launch a persistent search over a table of queries (count mode); q0 is
+// used when nq == 1.  kmax = largest motif in the table.
+int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int kmax, int grid,
+                 cudaStream_t stream);
+int table_occupancy(int kmax, int *blocks_per_sm);
 // Max resident blocks per SM for a given motif size / mode / block.
 int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm);
 

@@ -33,6 +33,17 @@ __global__ void pair_rec_kernel(const int *__restrict__ eids, const int4 *__rest
   }
 }
 
+// pair_loc[e] = {position of e in pair_rec, end of its run}
+__global__ void pair_loc_kernel(const int *__restrict__ eids, const int *__restrict__ starts,
+                                const int *__restrict__ lens, const int *__restrict__ num_runs,
+                                int2 *__restrict__ loc) {
+  const int P = *num_runs;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < P; r += gridDim.x * blockDim.x) {
+    const int b = starts[r], e = b + lens[r];
+    for (int i = b; i < e; i++) loc[eids[i]] = make_int2(i, e);
+  }
+}
+
 __global__ void pair_clear_kernel(int4 *__restrict__ tab, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -76,8 +87,9 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     g.pair_max_probe = 0;
     EVX_CUDA(cudaMalloc(&g.pair_tab, sizeof(int4)));
     EVX_CUDA(cudaMalloc(&g.pair_rec, sizeof(int2)));
+    EVX_CUDA(cudaMalloc(&g.pair_loc, sizeof(int2)));
     EVX_CUDA(cudaMemsetAsync(g.pair_tab, 0xff, sizeof(int4), s));
-    g.bytes += sizeof(int4) + sizeof(int2);
+    g.bytes += sizeof(int4) + 2 * sizeof(int2);
     return EVX_OK;
   }
   int sms = 148;
@@ -133,11 +145,13 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     g.pair_mask = (unsigned long long)(cap - 1);
     cudaError_t e = cudaMalloc(&g.pair_tab, sizeof(int4) * (size_t)cap);
     if (e == cudaSuccess) e = cudaMalloc(&g.pair_rec, sizeof(int2) * (size_t)n);
+    if (e == cudaSuccess) e = cudaMalloc(&g.pair_loc, sizeof(int2) * (size_t)n);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMalloc(pair index)"); goto cleanup; }
-    g.bytes += (int64_t)(sizeof(int4) * cap + sizeof(int2) * n);
+    g.bytes += (int64_t)(sizeof(int4) * cap + 2 * sizeof(int2) * n);
     EVX_CUDA(cudaMemsetAsync(ctr + 1, 0, 2 * sizeof(int), s));
     pair_clear_kernel<<<grid, block, 0, s>>>(g.pair_tab, cap);
     pair_rec_kernel<<<grid, block, 0, s>>>(vals_sorted, g.edges, g.pair_rec, n);
+    pair_loc_kernel<<<grid, block, 0, s>>>(vals_sorted, starts, lens, ctr, g.pair_loc);
     pair_insert_kernel<<<grid, block, 0, s>>>(ukeys, starts, lens, ctr, g.pair_tab, g.pair_mask, ctr + 1,
                                               ctr + 2);
     int h[2] = {0, 0};

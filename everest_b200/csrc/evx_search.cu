@@ -44,6 +44,9 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCap = 64;        // task slots per buffered level per warp
 constexpr int kBlock = 128;     // threads per block
 constexpr int kWarps = kBlock / 32;
+// resident blocks per SM the register budget aims for (deeper motifs keep
+// more per-level state live)
+constexpr int min_blocks(int k) { return k <= 3 ? 8 : (k == 4 ? 6 : 4); }
 
 template <int N>
 __device__ __forceinline__ int sel(const int (&a)[N], int i) {
@@ -96,6 +99,18 @@ __device__ __forceinline__ int pair_first_t_after(const GraphView &g, int lo, in
   return lo;
 }
 
+// Same, galloping up from lo (windows are usually a few entries long).
+__device__ __forceinline__ int pair_gallop_t_after(const GraphView &g, int lo, int hi, int tl) {
+  int step = 1;
+  while (lo < hi) {
+    const int probe = min(lo + step - 1, hi - 1);
+    if (__ldg(&g.pair_rec[probe].y) > tl) { hi = probe; break; }
+    lo = probe + 1;
+    step <<= 1;
+  }
+  return pair_first_t_after(g, lo, hi, tl);
+}
+
 // First index in [lo, hi) of pair_rec whose edge id (timestamp in strict
 // mode) is greater than key.
 __device__ __forceinline__ int pair_first_key_after(const GraphView &g, int lo, int hi, int key,
@@ -145,6 +160,7 @@ __device__ __forceinline__ int pair_window(const GraphView &g, int start, int le
 //   save[l][lane]     = scan state of level l parked while the warp descends
 template <int K>
 struct alignas(16) WarpSmem {
+  QueryDesc q;             // the warp's current query
   int4 root[32];
   int4 task[(K > 2) ? (K - 2) : 1][kCap][2];
   int4 save[(K > 2) ? (K - 2) : 1][32][2];
@@ -156,7 +172,7 @@ struct Prev {
   int eid, t, src, dst, pop, pip;
 };
 
-template <int K, bool ENUM>
+template <int K, bool ENUM, bool EXACT>
 struct Searcher {
   static constexpr int L = K - 1;          // levels; level l opens motif edge l + 1
   static constexpr int N = K + 1;          // motif nodes <= k + 1
@@ -164,18 +180,30 @@ struct Searcher {
   static constexpr int WIDE = ENUM ? 1 : 4;  // records per lane per last-level step
 
   const GraphView &g;
-  const MotifPlan &plan;
-  const SearchArgs &args;
+  const MotifPlan &plan;   // the current query's plan (per-warp copy in shared memory)
+  const EnumArgs &ea;
   WarpSmem<K> &sm;
   const int lane;
   const unsigned lt;
-  const int strict;
+  // the current query's options (reloaded when the warp switches queries)
+  int strict = 0, inline_last = 0, same_pair = 0, steal_interval = 0, min_split = 2, kq = K;
+  // motif edges of the current query: K itself when the launch has one
+  // motif size (EXACT), else the table entry's
+  __device__ __forceinline__ int kr() const { return EXACT ? K : kq; }
   unsigned long long cnt;
 
-  __device__ Searcher(const GraphView &g_, const MotifPlan &p_, const SearchArgs &a_, WarpSmem<K> &s_,
+  __device__ Searcher(const GraphView &g_, const MotifPlan &p_, const EnumArgs &e_, WarpSmem<K> &s_,
                       int lane_)
-      : g(g_), plan(p_), args(a_), sm(s_), lane(lane_), lt((1u << lane_) - 1u),
-        strict(a_.strict_ts), cnt(0) {}
+      : g(g_), plan(p_), ea(e_), sm(s_), lane(lane_), lt((1u << lane_) - 1u), cnt(0) {}
+
+  __device__ __forceinline__ void set_query(const QueryDesc &q) {
+    strict = (q.flags & kQStrict) ? 1 : 0;
+    inline_last = (q.flags & kQInlineLast) ? 1 : 0;
+    same_pair = (q.flags & kQSamePair) ? 1 : 0;
+    steal_interval = q.steal_interval;
+    min_split = q.min_split;
+    kq = q.plan.k;
+  }
 
   // Node images and edge ids of the partial match in slot s of level l.
   template <int l>
@@ -335,12 +363,12 @@ struct Searcher {
     }
 
     int steps = 0;
-    if constexpr (l == L - 1) {
+    if (l == kr() - 2 || l == L - 1) {
       // ------------------------------------------------ last level ----
       while (true) {
         const unsigned act = __ballot_sync(kFull, pos < end);
         if (!act) break;
-        if (act != kFull && args.steal_interval && ((++steps) & (args.steal_interval - 1)) == 0)
+        if (act != kFull && steal_interval && ((++steps) & (steal_interval - 1)) == 0)
           rebalance(act, pos, end, want, out, base, slot, root, tl, m, e);
         bool emit = false;
         int last_eid = 0;
@@ -365,17 +393,17 @@ struct Searcher {
         }
         if constexpr (ENUM) emit_row(emit, e, last_eid);
       }
-    } else {
+    } else if constexpr (l < L - 1) {
       // --------------------------------- scan, queue children, descend ----
       // The level before the last one counts a closing last edge inline by
       // range arithmetic on the pair index (count mode only).
-      const bool inline_last = (l == L - 2) && !ENUM && args.inline_last;
-      const int wl = plan.info[L - 1];
+      const bool inline_here = (l == kr() - 3) && !ENUM && (inline_last || same_pair);
+      const int wl = plan.info[kr() - 2];
       const int la = plan_a(wl), lb = plan_b(wl);
       int ca = -1, cb = -1, ctl = 0, cs = 0, cub = 0, ckey = 0;  // this lane's pair cursor
       while (true) {
         const unsigned act = __ballot_sync(kFull, pos < end);
-        if (!inline_last) {
+        if (!inline_here) {
           const int nb = sm.nb[l + 1];
           if (nb >= 32 || (!act && nb > 0)) {
             // park this level's state in shared memory while the warp descends,
@@ -394,7 +422,7 @@ struct Searcher {
           }
         }
         if (!act) break;
-        if (act != kFull && args.steal_interval && ((++steps) & (args.steal_interval - 1)) == 0)
+        if (act != kFull && steal_interval && ((++steps) & (steal_interval - 1)) == 0)
           rebalance(act, pos, end, want, out, base, slot, root, tl, m, e);
         bool push = false;
         int4 rc = make_int4(0, 0, 0, 0);
@@ -405,7 +433,16 @@ struct Searcher {
           if (rc.z > tl) pos = end;
           else push = structural_ok(rc.y, want, nmc, m);
         }
-        if (inline_last) {
+        if (inline_here && same_pair) {
+          if (push) {
+            // the last edge repeats this edge's endpoints: count the rest of
+            // the matched edge's own pair run inside the window
+            const int2 pl = __ldg(g.pair_loc + rc.x);
+            int lo = pl.x + 1;
+            if (strict) lo = pair_first_t_after(g, lo, pl.y, rc.z);
+            cnt += (unsigned long long)(pair_gallop_t_after(g, lo, pl.y, tl) - lo);
+          }
+        } else if (inline_here) {
           if (push) {
             // the last edge joins two nodes mapped before this level, so its
             // pair run is fixed for the task: keep a cursor into it that only
@@ -441,7 +478,7 @@ struct Searcher {
                                             int (&e)[EE]) {
     const int width = end - pos;
     const unsigned wmax = __reduce_max_sync(kFull, (unsigned)(width > 0 ? width : 0));
-    if ((int)wmax < args.min_split) return;
+    if ((int)wmax < min_split) return;
     const int donor = __ffs(__ballot_sync(kFull, (unsigned)width == wmax)) - 1;
     const unsigned idle = ~act;
     const int nthief = min(__popc(idle), (int)wmax - 1);
@@ -482,78 +519,118 @@ struct Searcher {
     if (!em) return;
     const int leader = __ffs(em) - 1;
     unsigned long long b0 = 0;
-    if (lane == leader) b0 = atomicAdd(args.count, (unsigned long long)__popc(em));
+    if (lane == leader) b0 = atomicAdd(ea.count, (unsigned long long)__popc(em));
     b0 = __shfl_sync(kFull, b0, leader);
     if (emit) {
       const unsigned long long s = b0 + (unsigned long long)__popc(em & lt);
-      if (s < (unsigned long long)args.cap) {
-        int *row = args.rows + s * K;
+      if (s < (unsigned long long)ea.cap) {
+        int *row = ea.rows + s * K;
 #pragma unroll
         for (int q = 0; q < K - 1; q++) row[q] = __ldg(g.euid + e[q < KE ? q : 0]);
         row[K - 1] = __ldg(g.euid + last_eid);
       }
-      if (!args.exact_total && s + 1 >= (unsigned long long)args.cap) atomicExch(args.stop, 1);
+      if (!ea.exact_total && s + 1 >= (unsigned long long)ea.cap) atomicExch(ea.stop, 1);
     }
   }
 };
 
-template <int K, bool ENUM>
-__global__ void __launch_bounds__(kBlock)
-search_kernel(const GraphView g, const MotifPlan plan, const SearchArgs args) {
+// Persistent search: warps claim root tiles from one work queue covering
+// every query of the launch, switch their per-warp query copy when a tile
+// belongs to another query, and add each query's count to counts[q].
+template <int K, bool ENUM, bool EXACT>
+__global__ void __launch_bounds__(kBlock, min_blocks(K))
+search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const LaunchArgs la,
+              const __grid_constant__ EnumArgs ea) {
   extern __shared__ int4 dyn_smem[];
   WarpSmem<K> *smem = reinterpret_cast<WarpSmem<K> *>(dyn_smem);
   const int lane = threadIdx.x & 31;
   WarpSmem<K> &sm = smem[threadIdx.x >> 5];
   if (lane < K) sm.nb[lane] = 0;
   __syncwarp();
-  Searcher<K, ENUM> S(g, plan, args, sm, lane);
-  const int batch = 32;
-  while (true) {
-    int b0 = 0;
-    if (lane == 0) {
-      if (ENUM && *(volatile int *)args.stop) b0 = args.root_end;
-      else b0 = atomicAdd(args.cursor, batch);
-    }
-    b0 = __shfl_sync(kFull, b0, 0);
-    if (b0 >= args.root_end) break;
-    const int r = b0 + lane;
-    bool has = false;
-    if (r < args.root_end) {
-      const int4 ed = __ldg(g.edges + r);
-      if (ed.x != ed.y) {  // self-loops are not roots
-        sm.root[lane] = make_int4(ed.x, ed.y, ed.z + args.delta, r);
-        has = true;
-      }
-    }
-    __syncwarp();
-    if (K == 2 && !ENUM && args.inline_last) {
-      // the only searched edge closes on the root's endpoints
-      if (has) {
-        const int4 rt = sm.root[lane];
-        const int w = plan.info[0];
-        const int ia = plan_a(w) == 0 ? rt.x : rt.y, ib = plan_b(w) == 0 ? rt.x : rt.y;
-        const int2 f = pair_find(g, ia, ib);
-        const int key = args.strict_ts ? rt.z - args.delta : rt.w;
-        S.cnt += (unsigned long long)pair_window(g, f.x, f.y, key, rt.z, args.strict_ts != 0);
-      }
-    } else {
-      S.template level<0>(has, lane, 32);
-    }
-    __syncwarp();
-  }
-  if (!ENUM) {
-    unsigned long long c = S.cnt;
+  Searcher<K, ENUM, EXACT> S(g, sm.q.plan, ea, sm, lane);
+  int cur_q = -1;
+  auto flush = [&]() {
+    if (!ENUM && cur_q >= 0) {
+      unsigned long long c = S.cnt;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
-    if (lane == 0 && c) atomicAdd(args.count, c);
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+      if (lane == 0 && c) atomicAdd(la.counts + cur_q, c);
+      S.cnt = 0;
+    }
+  };
+  while (true) {
+    int t = 0;
+    if (lane == 0) {
+      if (ENUM && *(volatile int *)ea.stop) t = la.total_tiles;
+      else t = atomicAdd(la.cursor, 1);
+    }
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= la.total_tiles) break;
+    // query of this tile
+    int q = 0;
+    if (la.table != nullptr && la.nq > 1) {
+      if (lane == 0) {
+        int lo = 0, hi = la.nq;  // last query with tile_beg <= t
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (__ldg(&la.table[mid].tile_beg) <= t) lo = mid; else hi = mid;
+        }
+        q = lo;
+      }
+      q = __shfl_sync(kFull, q, 0);
+    }
+    if (q != cur_q) {
+      flush();
+      // a query table in device memory when given (batches; replayable in a
+      // CUDA graph), else the single query passed by value
+      const int *src = (la.table != nullptr) ? reinterpret_cast<const int *>(la.table + q)
+                                             : reinterpret_cast<const int *>(&q0);
+      constexpr int W = sizeof(QueryDesc) / sizeof(int);
+      int *dst = reinterpret_cast<int *>(&sm.q);
+      for (int i = lane; i < W; i += 32) dst[i] = src[i];
+      __syncwarp();
+      S.set_query(sm.q);
+      cur_q = q;
+    }
+    const int rb = sm.q.root_beg + (t - sm.q.tile_beg) * la.tile_roots;
+    const int re = min(rb + la.tile_roots, sm.q.root_end);
+    const int delta = sm.q.delta;
+    for (int b0 = rb; b0 < re; b0 += 32) {
+      const int r = b0 + lane;
+      bool has = false;
+      if (r < re) {
+        const int4 ed = __ldg(g.edges + r);
+        if (ed.x != ed.y) {  // self-loops are not roots
+          sm.root[lane] = make_int4(ed.x, ed.y, ed.z + delta, r);
+          has = true;
+        }
+      }
+      __syncwarp();
+      if (!ENUM && S.kr() == 2 && S.inline_last) {
+        // the only searched edge closes on the root's endpoints
+        if (has) {
+          const int4 rt = sm.root[lane];
+          const int w = sm.q.plan.info[0];
+          const int ia = plan_a(w) == 0 ? rt.x : rt.y, ib = plan_b(w) == 0 ? rt.x : rt.y;
+          const int2 f = pair_find(g, ia, ib);
+          const int key = S.strict ? rt.z - delta : rt.w;
+          S.cnt += (unsigned long long)pair_window(g, f.x, f.y, key, rt.z, S.strict != 0);
+        }
+      } else {
+        S.template level<0>(has, lane, 32);
+      }
+      __syncwarp();
+      if (ENUM && *(volatile int *)ea.stop) break;
+    }
   }
+  flush();
 }
 
-template <int K, bool ENUM>
+template <int K, bool ENUM, bool EXACT>
 int setup_k() {
   static bool done = false;  // per process; the attribute is per function
   if (!done) {
-    cudaError_t e = cudaFuncSetAttribute(search_kernel<K, ENUM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(kWarps * sizeof(WarpSmem<K>)));
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
     done = true;
@@ -561,49 +638,107 @@ int setup_k() {
   return 0;
 }
 
-template <int K, bool ENUM>
-int launch_k(const GraphView &g, const MotifPlan &plan, const SearchArgs &args, int grid, int block,
+template <int K, bool ENUM, bool EXACT>
+int launch_k(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, const EnumArgs &ea, int grid,
              cudaStream_t s) {
-  (void)block;
-  int rc = setup_k<K, ENUM>();
+  int rc = setup_k<K, ENUM, EXACT>();
   if (rc) return rc;
-  search_kernel<K, ENUM><<<grid, kBlock, kWarps * sizeof(WarpSmem<K>), s>>>(g, plan, args);
+  search_kernel<K, ENUM, EXACT><<<grid, kBlock, kWarps * sizeof(WarpSmem<K>), s>>>(g, q0, la, ea);
   return 0;
 }
 
-template <int K, bool ENUM>
-int occ_k(int block, int *bps) {
-  (void)block;
-  int rc = setup_k<K, ENUM>();
+template <int K, bool ENUM, bool EXACT>
+int occ_k(int *bps) {
+  int rc = setup_k<K, ENUM, EXACT>();
   if (rc) return rc;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, search_kernel<K, ENUM>, kBlock,
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, search_kernel<K, ENUM, EXACT>, kBlock,
                                                                 kWarps * sizeof(WarpSmem<K>));
   return e == cudaSuccess ? 0 : cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
 }
 
+// Single-query launch description from the worker's SearchArgs.
+QueryDesc single_query(const MotifPlan &plan, const SearchArgs &args) {
+  QueryDesc q;
+  memset(&q, 0, sizeof(q));
+  q.plan = plan;
+  q.root_beg = args.root_beg;
+  q.root_end = args.root_end;
+  q.delta = args.delta;
+  q.flags = (args.strict_ts ? kQStrict : 0) | args.tail_flags;
+  q.steal_interval = args.steal_interval;
+  q.min_split = args.min_split;
+  q.tile_beg = 0;
+  return q;
+}
+
+constexpr int kSingleTileRoots = 64;
+
 }  // namespace
 
+// single-query launches: exact motif size, count or enumerate
 #define EVX_K_DISPATCH(FN, ...)                                        \
   switch (k) {                                                         \
-    case 2: return enumerate ? FN<2, true>(__VA_ARGS__) : FN<2, false>(__VA_ARGS__); \
-    case 3: return enumerate ? FN<3, true>(__VA_ARGS__) : FN<3, false>(__VA_ARGS__); \
-    case 4: return enumerate ? FN<4, true>(__VA_ARGS__) : FN<4, false>(__VA_ARGS__); \
-    case 5: return enumerate ? FN<5, true>(__VA_ARGS__) : FN<5, false>(__VA_ARGS__); \
-    case 6: return enumerate ? FN<6, true>(__VA_ARGS__) : FN<6, false>(__VA_ARGS__); \
-    case 7: return enumerate ? FN<7, true>(__VA_ARGS__) : FN<7, false>(__VA_ARGS__); \
-    case 8: return enumerate ? FN<8, true>(__VA_ARGS__) : FN<8, false>(__VA_ARGS__); \
+    case 2: return enumerate ? FN<2, true, true>(__VA_ARGS__) : FN<2, false, true>(__VA_ARGS__); \
+    case 3: return enumerate ? FN<3, true, true>(__VA_ARGS__) : FN<3, false, true>(__VA_ARGS__); \
+    case 4: return enumerate ? FN<4, true, true>(__VA_ARGS__) : FN<4, false, true>(__VA_ARGS__); \
+    case 5: return enumerate ? FN<5, true, true>(__VA_ARGS__) : FN<5, false, true>(__VA_ARGS__); \
+    case 6: return enumerate ? FN<6, true, true>(__VA_ARGS__) : FN<6, false, true>(__VA_ARGS__); \
+    case 7: return enumerate ? FN<7, true, true>(__VA_ARGS__) : FN<7, false, true>(__VA_ARGS__); \
+    case 8: return enumerate ? FN<8, true, true>(__VA_ARGS__) : FN<8, false, true>(__VA_ARGS__); \
+    default: return fail(EVX_ERR_INVALID, "motif edge count out of range");          \
+  }
+// query tables: count mode, motif sizes up to kmax
+#define EVX_T_DISPATCH(FN, ...)                                        \
+  switch (k) {                                                         \
+    case 2: return FN<2, false, false>(__VA_ARGS__);                   \
+    case 3: return FN<3, false, false>(__VA_ARGS__);                   \
+    case 4: return FN<4, false, false>(__VA_ARGS__);                   \
+    case 5: return FN<5, false, false>(__VA_ARGS__);                   \
+    case 6: return FN<6, false, false>(__VA_ARGS__);                   \
+    case 7: return FN<7, false, false>(__VA_ARGS__);                   \
+    case 8: return FN<8, false, false>(__VA_ARGS__);                   \
     default: return fail(EVX_ERR_INVALID, "motif edge count out of range");          \
   }
 
 int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &args, int grid, int block,
                   cudaStream_t stream) {
+  (void)block;
   const int k = plan.k;
   const bool enumerate = args.enumerate != 0;
-  EVX_K_DISPATCH(launch_k, g, plan, args, grid, block, stream)
+  const QueryDesc q0 = single_query(plan, args);
+  LaunchArgs la;
+  la.table = nullptr;
+  la.nq = 1;
+  la.tile_roots = kSingleTileRoots;
+  const int n = args.root_end - args.root_beg;
+  la.total_tiles = n > 0 ? (n + kSingleTileRoots - 1) / kSingleTileRoots : 0;
+  la.cursor = args.cursor;
+  la.counts = args.count;
+  EnumArgs ea;
+  ea.rows = args.rows;
+  ea.cap = args.cap;
+  ea.exact_total = args.exact_total;
+  ea.stop = args.stop;
+  ea.count = args.count;
+  EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
+}
+
+int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int kmax, int grid,
+                 cudaStream_t stream) {
+  const int k = kmax;
+  EnumArgs ea;
+  memset(&ea, 0, sizeof(ea));
+  EVX_T_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
 }
 
 int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm) {
-  EVX_K_DISPATCH(occ_k, block, blocks_per_sm)
+  (void)block;
+  EVX_K_DISPATCH(occ_k, blocks_per_sm)
+}
+
+int table_occupancy(int kmax, int *blocks_per_sm) {
+  const int k = kmax;
+  EVX_T_DISPATCH(occ_k, blocks_per_sm)
 }
 
 int search_block_size() { return kBlock; }

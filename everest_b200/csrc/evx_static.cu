@@ -99,12 +99,7 @@ extern "C" int evx_count_static(const evx_graph *gh, int nq, const int *k, const
     a.steal_interval = (flags & EVX_FLAG_NO_STEAL) ? 0 : 16;
     a.min_split = 2;
     a.enumerate = 0;
-    {
-      const int wl = plan.info[kq - 2];
-      const int nm_prev = (kq >= 3) ? plan_nm(plan.info[kq - 3]) : 2;
-      const bool fixed_pair = plan_a(wl) < nm_prev && plan_b(wl) < nm_prev;
-      a.inline_last = (!(flags & EVX_FLAG_NO_PAIR_INDEX) && plan_kind(wl) == 2 && fixed_pair) ? 1 : 0;
-    }
+    a.tail_flags = tail_mode(plan, flags, false);
     a.count = scratch + q;
     a.cursor = reinterpret_cast<int *>(scratch + EVX_STATIC_MAX_QUERIES + q);
     a.stop = a.cursor + 1;
@@ -115,7 +110,7 @@ extern "C" int evx_count_static(const evx_graph *gh, int nq, const int *k, const
     const int grid = bps * sms;
     if ((int64_t)a.root_end + (int64_t)grid * 4 * 32 >= (int64_t)INT_MAX)
       return fail(EVX_ERR_OVERFLOW, "root cursor would overflow int32");
-    static_reset_kernel<<<1, 1, 0, s>>>(q, a.root_beg);
+    static_reset_kernel<<<1, 1, 0, s>>>(q, 0);  // the work queue counts root tiles from 0
     EVX_CUDA(cudaGetLastError());
     if (a.root_end > a.root_beg) {
       rc = launch_search(view, plan, a, grid, 128, s);

@@ -162,6 +162,31 @@ EVX_API int evx_worker_set_tuning(evx_worker *w, int block, int blocks_per_sm,
  * and device milliseconds measured with CUDA events around them. */
 EVX_API int evx_worker_last_stats(evx_worker *w, int *kernel_launches, float *device_ms);
 
+/* -------------------------------------------------------------- batches --
+ * Many count queries against one resident graph in a single persistent
+ * launch (no counterpart in the reference, whose batch driver re-generates,
+ * re-compiles and re-launches per query, system/batch-query.py:14-20 and
+ * system/tmine/frontend.py:135-143).  Queries' root ranges are cut into
+ * tiles that form one device work queue.  The launch sequence is captured
+ * in a CUDA graph and replayed while the batch keeps its shape. */
+typedef struct evx_batch evx_batch;
+EVX_API int evx_batch_create(int device, int max_queries, void *stream, evx_batch **out);
+EVX_API int evx_batch_destroy(evx_batch *b);
+/* Add one count query (all queries of a batch use one graph); *index = its
+ * position in the result array. */
+EVX_API int evx_batch_add(evx_batch *b, const evx_graph *g, int k, const int *mu, const int *mv,
+                          int delta, int64_t beg, int64_t end, unsigned flags, int *index);
+EVX_API int evx_batch_clear(evx_batch *b);
+EVX_API int evx_batch_launch(evx_batch *b);
+/* Wait for the launched batch; counts[i] for the first n queries. */
+EVX_API int evx_batch_result(evx_batch *b, uint64_t *counts, int n);
+EVX_API int evx_batch_run(evx_batch *b, uint64_t *counts, int n);
+/* tile_roots (multiple of 32), blocks per SM (0 = occupancy), steal
+ * interval, min split, use_graph (capture + replay), reserved. */
+EVX_API int evx_batch_set_tuning(evx_batch *b, int tile_roots, int blocks_per_sm, int steal_interval,
+                                 int min_split, int use_graph, int reserved);
+EVX_API int evx_batch_last_stats(evx_batch *b, int *kernel_launches, float *device_ms);
+
 /* ------------------------------------------------- allocation-free count --
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * at query time (device memory fully reserved by another allocator, or a
