@@ -36,6 +36,7 @@ EXPORTS = [
     "evx_worker_last_stats", "evx_host_register", "evx_host_unregister", "evx_count_static",
     "evx_batch_create", "evx_batch_destroy", "evx_batch_add", "evx_batch_clear", "evx_batch_launch",
     "evx_batch_result", "evx_batch_run", "evx_batch_set_tuning", "evx_batch_last_stats",
+    "evx_device_mem_info", "evx_worker_query", "evx_batch_query",
 ]
 STATIC_MAX_QUERIES = 256
 
@@ -65,6 +66,9 @@ def lib():
         sig = {
             "evx_last_error": ([], ctypes.c_char_p),
             "evx_device_count": ([_PI], _I),
+            "evx_device_mem_info": ([_I, _PI64, _PI64], _I),
+            "evx_worker_query": ([_P, _PI], _I),
+            "evx_batch_query": ([_P, _PI], _I),
             "evx_edgelist_parse": ([ctypes.c_char_p, _PI64, _PPI, _PPI, _PPI, _PPI], _I),
             "evx_graph_build_host": ([_P, _P, _P, _P, _I64, _I64, _PI64, _PI64,
                                       _PPI, _PPI, _PPI, _PPI, _PPI, _PPI], _I),
@@ -121,6 +125,13 @@ def device_count() -> int:
     n = ctypes.c_int(0)
     check(lib().evx_device_count(ctypes.byref(n)))
     return n.value
+
+
+def device_mem_info(device: int = 0):
+    """(free, total) device memory in bytes."""
+    fr, tot = ctypes.c_int64(0), ctypes.c_int64(0)
+    check(lib().evx_device_mem_info(int(device), ctypes.byref(fr), ctypes.byref(tot)))
+    return fr.value, tot.value
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -358,6 +369,12 @@ class Worker:
         check(lib().evx_worker_result(self._h, ctypes.byref(c)))
         return int(c.value)
 
+    def done(self) -> bool:
+        """True once the launched search has finished (never blocks)."""
+        d = ctypes.c_int(0)
+        check(lib().evx_worker_query(self._h, ctypes.byref(d)))
+        return bool(d.value)
+
     def enum_rows(self, n: int) -> np.ndarray:
         n = max(0, int(n))
         buf = np.zeros((max(n, 1), max(self.k, 1)), np.int32)
@@ -422,6 +439,11 @@ class Batch:
     def run(self):
         self.launch()
         return self.result()
+
+    def done(self) -> bool:
+        d = ctypes.c_int(0)
+        check(lib().evx_batch_query(self._h, ctypes.byref(d)))
+        return bool(d.value)
 
     def last_stats(self):
         n = ctypes.c_int()

@@ -257,6 +257,16 @@ int evx_batch_result(evx_batch *b, uint64_t *counts, int n) {
   return EVX_OK;
 }
 
+int evx_batch_query(evx_batch *b, int *done) {
+  if (!b || !done) return fail(EVX_ERR_INVALID, "null argument");
+  if (!b->launched) return fail(EVX_ERR_STATE, "query before launch");
+  cudaError_t e = cudaEventQuery(b->ev1);
+  if (e == cudaErrorNotReady) { *done = 0; return EVX_OK; }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventQuery");
+  *done = 1;
+  return EVX_OK;
+}
+
 int evx_batch_run(evx_batch *b, uint64_t *counts, int n) {
   int rc = evx_batch_launch(b);
   if (rc) return rc;

@@ -116,6 +116,19 @@ extern "C" {
 
 const char *evx_last_error(void) { return g_last_error.c_str(); }
 
+int evx_device_mem_info(int device, int64_t *free_bytes, int64_t *total_bytes) {
+  int ndev = 0;
+  evx_device_count(&ndev);
+  if (ndev == 0) return fail(EVX_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= ndev) return fail(EVX_ERR_INVALID, "bad device index");
+  EVX_CUDA(cudaSetDevice(device));
+  size_t fr = 0, tot = 0;
+  EVX_CUDA(cudaMemGetInfo(&fr, &tot));
+  if (free_bytes) *free_bytes = (int64_t)fr;
+  if (total_bytes) *total_bytes = (int64_t)tot;
+  return EVX_OK;
+}
+
 int evx_host_register(void *ptr, int64_t bytes) {
   if (!ptr || bytes <= 0) return fail(EVX_ERR_INVALID, "bad host range");
   EVX_CUDA(cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault));
@@ -465,6 +478,16 @@ int evx_worker_result(evx_worker *w, uint64_t *count) {
   w->last_count = *w->count_h;
   *count = w->last_count;
   w->launched = false;
+  return EVX_OK;
+}
+
+int evx_worker_query(evx_worker *w, int *done) {
+  if (!w || !done) return fail(EVX_ERR_INVALID, "null argument");
+  if (!w->launched) return fail(EVX_ERR_STATE, "query before launch");
+  cudaError_t e = cudaEventQuery(w->ev1);
+  if (e == cudaErrorNotReady) { *done = 0; return EVX_OK; }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventQuery");
+  *done = 1;
   return EVX_OK;
 }
 

@@ -1,0 +1,230 @@
+"""Serving loop: continuous batching of motif queries on resident graphs.
+
+The reference answers one query at a time and re-uploads the graph for each
+(system/tmine/frontend.py:69-96, system/batch-query.py:14-20).  Here:
+
+* graphs stay resident on the device (``add_graph``);
+* ``submit`` returns a future immediately; a loop thread admits requests:
+  - count queries are packed into batches (one persistent launch each, see
+    ``capi.Batch``); up to ``inflight_batches`` batches run at once on their
+    own streams, so requests that arrive while others are on the GPU are
+    admitted as soon as a batch slot frees up;
+  - enumerate queries run as single-query searches on their own streams,
+    admitted only when the device has room for their row buffers
+    (cap x k x 4 bytes plus a reserve) and an enumeration slot is free;
+* completed work is detected without blocking (CUDA event queries), futures
+  are resolved and each request's latency (submit -> result) is recorded.
+
+Results are independent of the mix: every query keeps its own counters in
+the batch (one per query) or its own worker.
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import capi
+
+
+@dataclass
+class Request:
+    graph: str
+    mu: Sequence[int]
+    mv: Sequence[int]
+    delta: int
+    enum_cap: int = 0
+    flags: int = 0
+    submitted: float = field(default_factory=time.perf_counter)
+    future: Future = field(default_factory=Future)
+
+
+@dataclass
+class Result:
+    count: int
+    rows: Optional[np.ndarray] = None
+    latency_s: float = 0.0
+
+
+class Server:
+    def __init__(self, device: int = 0, max_batch: int = 64, inflight_batches: int = 2,
+                 enum_slots: int = 2, mem_reserve: int = 1 << 30, idle_sleep_s: float = 50e-6,
+                 backend=None):
+        # backend: the module providing Batch, Worker, DeviceGraph and
+        # device_mem_info (the C-ABI binding; tests substitute a fake)
+        self.be = backend if backend is not None else capi
+        capi_ = self.be
+        self.device = device
+        self.max_batch = max_batch
+        self.mem_reserve = mem_reserve
+        self.idle_sleep_s = idle_sleep_s
+        self.graphs: Dict[str, capi.DeviceGraph] = {}
+        self.count_q: "collections.deque[Request]" = collections.deque()
+        self.enum_q: "collections.deque[Request]" = collections.deque()
+        self.lock = threading.Lock()
+        self.cv = threading.Condition(self.lock)
+        self.batches = [capi_.Batch(device, max_batch) for _ in range(inflight_batches)]
+        self.batch_reqs: List[Optional[List[Request]]] = [None] * inflight_batches
+        self.enum_workers = [capi_.Worker(device) for _ in range(enum_slots)]
+        self.enum_reqs: List[Optional[Request]] = [None] * enum_slots
+        self.latencies: List[float] = []
+        self.completed = 0
+        self.batches_launched = 0
+        self.first_submit: Optional[float] = None
+        self.last_done: Optional[float] = None
+        self.error: Optional[BaseException] = None
+        self.running = True
+        self.thread = threading.Thread(target=self._loop, name="evx-serve", daemon=True)
+        self.thread.start()
+
+    # ------------------------------------------------------------- API --
+    def add_graph(self, name: str, host: capi.HostGraph) -> None:
+        self.graphs[name] = self.be.DeviceGraph(host, self.device)
+
+    def submit(self, graph: str, mu, mv, delta: int, enum_cap: int = 0, flags: int = 0) -> Future:
+        if graph not in self.graphs:
+            raise KeyError(f"graph {graph!r} is not resident")
+        r = Request(graph, list(mu), list(mv), int(delta), int(enum_cap), int(flags))
+        with self.cv:
+            if self.first_submit is None:
+                self.first_submit = r.submitted
+            (self.enum_q if enum_cap > 0 else self.count_q).append(r)
+            self.cv.notify()
+        return r.future
+
+    def stats(self) -> dict:
+        lat = np.array(self.latencies) if self.latencies else np.zeros(1)
+        span = (self.last_done - self.first_submit) if (self.last_done and self.first_submit) else 0.0
+        return {"completed": self.completed, "batches": self.batches_launched,
+                "queries_per_s": self.completed / span if span > 0 else 0.0,
+                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                "p999_ms": float(np.percentile(lat, 99.9) * 1e3), "max_ms": float(lat.max() * 1e3)}
+
+    def drain(self, timeout_s: float = 600.0) -> None:
+        t0 = time.time()
+        while True:
+            with self.lock:
+                busy = (self.count_q or self.enum_q or any(self.batch_reqs) or any(self.enum_reqs))
+            if not busy:
+                return
+            if self.error:
+                raise self.error
+            if time.time() - t0 > timeout_s:
+                raise TimeoutError("serving queue did not drain")
+            time.sleep(0.001)
+
+    def close(self) -> None:
+        with self.cv:
+            self.running = False
+            self.cv.notify()
+        self.thread.join(timeout=60)
+        for b in self.batches:
+            b.close()
+        for w in self.enum_workers:
+            w.close()
+        for g in self.graphs.values():
+            if hasattr(g, "free"):
+                g.free()
+        self.graphs.clear()
+
+    # ------------------------------------------------------------ loop --
+    def _finish(self, r: Request, res: Result) -> None:
+        now = time.perf_counter()
+        res.latency_s = now - r.submitted
+        self.latencies.append(res.latency_s)
+        self.completed += 1
+        self.last_done = now
+        r.future.set_result(res)
+
+    def _poll(self) -> bool:
+        progressed = False
+        for i, b in enumerate(self.batches):
+            reqs = self.batch_reqs[i]
+            if reqs is not None and b.done():
+                counts = b.result()
+                b.clear()
+                self.batch_reqs[i] = None
+                for r, c in zip(reqs, counts):
+                    self._finish(r, Result(c))
+                progressed = True
+        for i, w in enumerate(self.enum_workers):
+            r = self.enum_reqs[i]
+            if r is not None and w.done():
+                c = w.result()
+                rows = w.enum_rows(r.enum_cap)
+                self.enum_reqs[i] = None
+                self._finish(r, Result(c, rows))
+                progressed = True
+        return progressed
+
+    def _admit(self) -> bool:
+        progressed = False
+        # count queries: fill free batch slots (one graph per batch)
+        for i, b in enumerate(self.batches):
+            if self.batch_reqs[i] is not None:
+                continue
+            with self.lock:
+                if not self.count_q:
+                    break
+                g = self.count_q[0].graph
+                take = []
+                rest = collections.deque()
+                while self.count_q and len(take) < self.max_batch:
+                    r = self.count_q.popleft()
+                    (take if r.graph == g else rest).append(r)
+                rest.extend(self.count_q)
+                self.count_q = rest
+            for r in take:
+                b.add(self.graphs[r.graph], r.mu, r.mv, r.delta, 0, -1, r.flags)
+            b.launch()
+            self.batch_reqs[i] = take
+            self.batches_launched += 1
+            progressed = True
+        # enumerate queries: admission by the memory their row buffers need
+        for i, w in enumerate(self.enum_workers):
+            if self.enum_reqs[i] is not None:
+                continue
+            with self.lock:
+                if not self.enum_q:
+                    break
+                r = self.enum_q[0]
+            need = r.enum_cap * len(r.mu) * 4
+            free, _ = self.be.device_mem_info(self.device)
+            if need + self.mem_reserve > free:
+                break  # wait for running work to release memory
+            with self.lock:
+                self.enum_q.popleft()
+            w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, 0, -1, r.enum_cap, r.flags)
+            w.launch()
+            self.enum_reqs[i] = r
+            progressed = True
+        return progressed
+
+    def _loop(self) -> None:
+        try:
+            while True:
+                with self.cv:
+                    if not self.running:
+                        return
+                    idle = not (self.count_q or self.enum_q or any(self.batch_reqs) or any(self.enum_reqs))
+                    if idle:
+                        self.cv.wait(timeout=0.05)
+                        continue
+                p1 = self._poll()
+                p2 = self._admit()
+                if not (p1 or p2):
+                    time.sleep(self.idle_sleep_s)
+        except BaseException as e:  # surface loop failures to callers
+            self.error = e
+            with self.lock:
+                pending = list(self.count_q) + list(self.enum_q)
+                pending += [r for reqs in self.batch_reqs if reqs for r in reqs]
+                pending += [r for r in self.enum_reqs if r]
+            for r in pending:
+                if not r.future.done():
+                    r.future.set_exception(e)

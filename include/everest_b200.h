@@ -54,6 +54,9 @@ EVX_API const char *evx_last_error(void);
 /* Number of visible CUDA devices (0 when none). */
 EVX_API int evx_device_count(int *count);
 
+/* Free and total device memory in bytes (admission of enumeration buffers). */
+EVX_API int evx_device_mem_info(int device, int64_t *free_bytes, int64_t *total_bytes);
+
 /* ------------------------------------------------------------ host data --
  * Edge-list loading (replaces EdgeListLoader::createEdgeListCache,
  * src/core/cpu/data.cc:175-290): parse "u v t" lines with atoi semantics,
@@ -146,6 +149,8 @@ EVX_API int evx_worker_run(evx_worker *w, uint64_t *count);
  * stream; evx_worker_result synchronises and returns the count. */
 EVX_API int evx_worker_launch(evx_worker *w);
 EVX_API int evx_worker_result(evx_worker *w, uint64_t *count);
+/* *done = 1 when the launched search has finished (never blocks). */
+EVX_API int evx_worker_query(evx_worker *w, int *done);
 
 /* Copy min(n, rows found, cap) enumeration rows (k ints each: the original
  * line ids of e_0..e_{k-1}) to host memory (replaces
@@ -181,6 +186,8 @@ EVX_API int evx_batch_launch(evx_batch *b);
 /* Wait for the launched batch; counts[i] for the first n queries. */
 EVX_API int evx_batch_result(evx_batch *b, uint64_t *counts, int n);
 EVX_API int evx_batch_run(evx_batch *b, uint64_t *counts, int n);
+/* *done = 1 when the launched batch has finished (never blocks). */
+EVX_API int evx_batch_query(evx_batch *b, int *done);
 /* tile_roots (multiple of 32), blocks per SM (0 = occupancy), steal
  * interval, min split, use_graph (capture + replay), reserved. */
 EVX_API int evx_batch_set_tuning(evx_batch *b, int tile_roots, int blocks_per_sm, int steal_interval,

@@ -1,0 +1,137 @@
+"""Serving-loop admission logic on CPU with a fake device backend (the
+oracle computes the counts; the backend only models slots, completion and
+free memory)."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from everest_b200 import serve, synth
+from oracle import oracle as O
+
+
+class FakeBackend:
+    """Batch / Worker / DeviceGraph / device_mem_info with host semantics."""
+
+    def __init__(self, graphs, free_bytes):
+        self.graphs = graphs          # name -> oracle Graph
+        self.free = free_bytes
+        self.lock = threading.Lock()
+        self.max_concurrent_enum = 0
+        self.running_enum = 0
+
+    def device_mem_info(self, device):
+        with self.lock:
+            return self.free, 1 << 40
+
+    def DeviceGraph(self, host, device):
+        return host  # the test passes the graph name as "host"
+
+    def Batch(self, device, max_q):
+        be = self
+
+        class B:
+            def __init__(self):
+                self.q = []
+                self.t_done = None
+
+            def add(self, g, mu, mv, d, beg, end, flags):
+                self.q.append((g, mu, mv, d))
+
+            def launch(self):
+                self.res = [O.count(be.graphs[g], mu, mv, d)[0] for g, mu, mv, d in self.q]
+                self.t_done = time.perf_counter() + 0.002
+
+            def done(self):
+                return time.perf_counter() >= self.t_done
+
+            def result(self):
+                return self.res
+
+            def clear(self):
+                self.q = []
+
+            def close(self):
+                pass
+        return B()
+
+    def Worker(self, device):
+        be = self
+
+        class W:
+            def take(self, g, mu, mv, d, beg, end, cap, flags):
+                self.args = (g, mu, mv, d, cap)
+
+            def launch(self):
+                g, mu, mv, d, cap = self.args
+                with be.lock:
+                    be.free -= cap * len(mu) * 4
+                    be.running_enum += 1
+                    be.max_concurrent_enum = max(be.max_concurrent_enum, be.running_enum)
+                self.rows, self.total = O.enumerate_rows(be.graphs[g], mu, mv, d, cap)
+                self.t_done = time.perf_counter() + 0.003
+
+            def done(self):
+                return time.perf_counter() >= self.t_done
+
+            def result(self):
+                g, mu, mv, d, cap = self.args
+                with be.lock:
+                    be.free += cap * len(mu) * 4
+                    be.running_enum -= 1
+                return min(self.total, self.total)
+
+            def enum_rows(self, n):
+                return self.rows[:n]
+
+            def close(self):
+                pass
+        return W()
+
+
+@pytest.fixture(scope="module")
+def graph():
+    spec = synth.GraphSpec("serve-zipf", "zipf", 200, 3000, seed=6, t_max=30_000)
+    u, v, t = synth.generate(spec)
+    return O.Graph(u, v, t, spec.num_nodes)
+
+
+def test_results_same_alone_and_in_mix(graph):
+    be = FakeBackend({"g": graph}, free_bytes=1 << 40)
+    srv = serve.Server(max_batch=8, inflight_batches=2, enum_slots=2, mem_reserve=0, backend=be)
+    srv.add_graph("g", "g")
+    qs = [([0, 1, 2], [1, 2, 0], 2000), ([0, 0, 0], [1, 2, 1], 3000), ([0, 1], [1, 0], 4000),
+          ([0, 1, 2, 3], [1, 2, 3, 0], 3000)] * 6
+    futs = [srv.submit("g", mu, mv, d) for mu, mv, d in qs]
+    efut = srv.submit("g", [0, 1, 2], [1, 2, 0], 2000, enum_cap=50)
+    srv.drain(60)
+    for (mu, mv, d), f in zip(qs, futs):
+        assert f.result(1).count == O.count(graph, mu, mv, d)[0]
+    er = efut.result(1)
+    assert er.rows.shape[0] == min(50, O.count(graph, [0, 1, 2], [1, 2, 0], 2000)[0])
+    st = srv.stats()
+    assert st["completed"] == len(qs) + 1 and st["batches"] >= len(qs) // 8
+    assert st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
+    srv.close()
+
+
+def test_enumeration_admission_waits_for_memory(graph):
+    # room for one enumeration buffer at a time
+    cap = 1000
+    be = FakeBackend({"g": graph}, free_bytes=cap * 3 * 4 + 100)
+    srv = serve.Server(max_batch=4, inflight_batches=1, enum_slots=3, mem_reserve=50, backend=be)
+    srv.add_graph("g", "g")
+    futs = [srv.submit("g", [0, 1, 2], [1, 2, 0], 1000 + 500 * i, enum_cap=cap) for i in range(5)]
+    srv.drain(60)
+    assert all(f.result(1).count >= 0 for f in futs)
+    assert be.max_concurrent_enum == 1
+    srv.close()
+
+
+def test_unknown_graph_rejected(graph):
+    be = FakeBackend({"g": graph}, free_bytes=1 << 40)
+    srv = serve.Server(backend=be)
+    with pytest.raises(KeyError):
+        srv.submit("nope", [0, 1], [1, 0], 5)
+    srv.close()
