@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--impl", default="evx", choices=["evx", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="default launch parameters instead of per-query autotuned ones")
     ap.add_argument("--single-query", type=int, default=-1,
                     help="profiling aid: run only query I of the workload --reps times and exit")
     ap.add_argument("--reps", type=int, default=2)
@@ -242,8 +244,18 @@ def run_gpu_arm(args):
     sh = stream.cuda_stream
     dg = capi.DeviceGraph(host, dev, sh)
     workers = [capi.Worker(dev, sh) for _ in qs]
-    for w, q in zip(workers, qs):
-        w.take(dg, q["mu"], q["mv"], q["delta"])
+    flags = [0] * len(qs)
+    tuned = {}
+    if not args.no_autotune:
+        # per-query launch parameters, tuned on a root sample before timing
+        from everest_b200 import autotune
+        tuner = autotune.Autotuner(dev, sample_roots=400_000)
+        for i, (w, q) in enumerate(zip(workers, qs)):
+            cfg = tuner.tune(dg, q["mu"], q["mv"], q["delta"], w)
+            flags[i] = autotune.Autotuner.apply(w, cfg)
+            tuned[q["name"]] = {k: cfg[k] for k in ("blocks_per_sm", "steal_interval", "min_split", "flags")}
+    for w, q, f in zip(workers, qs, flags):
+        w.take(dg, q["mu"], q["mv"], q["delta"], 0, -1, 0, f)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
 
     def barrier():
@@ -291,8 +303,8 @@ def run_gpu_arm(args):
             ev1 = torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
             g2 = capi.DeviceGraph(host, dev, sh)
-            for w, q in zip(workers, qs):
-                w.take(g2, q["mu"], q["mv"], q["delta"])
+            for w, q, f in zip(workers, qs, flags):
+                w.take(g2, q["mu"], q["mv"], q["delta"], 0, -1, 0, f)
                 w.launch()
             cs = [w.result() for w in workers]
             ev1.record(stream)
@@ -328,7 +340,9 @@ def run_gpu_arm(args):
                    "graph_edges": host.num_edges, "graph_vertices": host.num_vertices,
                    "queries_per_step": len(qs), "matches_per_step": matches,
                    "l2": "flushed before every step (256 MB write)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "autotune": "per-query, root sample of 400k, outside the timed region"
+                   if tuned else "off"},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e_total / args.steps},
         "gpu_launches": launches,

@@ -13,7 +13,7 @@ from typing import Optional, Sequence, Tuple
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "libeverest_b200.so")
+LIB_PATH = os.environ.get("EVX_LIB_PATH") or os.path.join(PKG, "libeverest_b200.so")
 
 EVX_OK = 0
 EVX_ERR = {
@@ -24,6 +24,7 @@ FLAG_STRICT_TS = 1
 FLAG_EXACT_TOTAL = 2
 FLAG_NO_STEAL = 4
 FLAG_NO_PAIR_INDEX = 8
+FLAG_PAIR_DIR = 16
 MAX_MOTIF_EDGES = 8
 
 # every symbol include/everest_b200.h declares

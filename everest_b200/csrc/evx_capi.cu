@@ -28,6 +28,37 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 int graph_t_range(DeviceGraph &g, int *scratch_d, cudaStream_t s);
 
+namespace {
+std::mutex g_pool_mu;
+cudaMemPool_t g_pools[64] = {};
+}  // namespace
+
+cudaError_t dev_alloc(void **p, size_t bytes, int device, cudaStream_t s) {
+  if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+  cudaMemPool_t pool;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[device]) {
+      cudaMemPoolProps props;
+      std::memset(&props, 0, sizeof(props));
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = device;
+      cudaError_t e = cudaMemPoolCreate(&g_pools[device], &props);
+      if (e != cudaSuccess) return e;
+      uint64_t keep = ~0ull;  // keep freed memory mapped for reuse
+      e = cudaMemPoolSetAttribute(g_pools[device], cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+    }
+    pool = g_pools[device];
+  }
+  return cudaMallocFromPoolAsync(p, bytes ? bytes : 1, pool, s);
+}
+
+void dev_free(void *p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
 // Decode a relabeled motif into the per-level plan (HostMotifData rules,
 // src/core/cpu/data.cc:416-446).
 int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
@@ -65,10 +96,11 @@ int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
 }
 
 // Range arithmetic on the pair index replaces the last level's scan (count
-// mode) when the last edge closes on two nodes mapped before the
-// second-to-last edge (its pair is fixed per partial match: kQInlineLast),
-// or repeats the second-to-last edge's endpoints (its pair run is the one
-// the matched edge sits in: kQSamePair).
+// mode) for a closing last edge: when it closes on two nodes mapped before
+// the second-to-last edge (its pair is fixed per partial match:
+// kQInlineLast), when it repeats the second-to-last edge's endpoints (its
+// pair run is the one the matched edge sits in: kQSamePair), and, on
+// request, through the per-node pair directory (kQPairDir).
 int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
   const int k = plan.k;
   if (enumerate || (flags & EVX_FLAG_NO_PAIR_INDEX) || k < 2) return 0;
@@ -79,6 +111,8 @@ int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
   if (k >= 3) {
     const int wp = plan.info[k - 3];
     if (plan_a(wp) == plan_a(wl) && plan_b(wp) == plan_b(wl)) return kQSamePair;
+    // the pair depends on the node the second-to-last edge maps
+    if (flags & EVX_FLAG_PAIR_DIR) return kQPairDir;
   }
   return 0;
 }
@@ -173,7 +207,7 @@ static int alloc_graph(int device, int64_t E, int64_t V, evx_graph **out, cudaSt
   size_t bytes = 0;
   cudaError_t err = cudaSuccess;
   auto A = [&](void **p, size_t n) {
-    if (err == cudaSuccess) { err = cudaMalloc(p, n); bytes += n; }
+    if (err == cudaSuccess) { err = dev_alloc(p, n, device, s); bytes += n; }
   };
   A((void **)&g.edges, sizeof(int4) * e1);
   A((void **)&g.inpos, sizeof(int) * e1);
@@ -183,21 +217,21 @@ static int alloc_graph(int device, int64_t E, int64_t V, evx_graph **out, cudaSt
   A((void **)&g.node_rng, sizeof(int4) * (size_t)(V > 0 ? V : 1));
   g.bytes = (int64_t)bytes;
   if (err != cudaSuccess) {
-    cudaFree(g.edges); cudaFree(g.inpos); cudaFree(g.euid); cudaFree(g.out_rec);
-    cudaFree(g.in_rec); cudaFree(g.node_rng);
+    dev_free(g.edges, s); dev_free(g.inpos, s); dev_free(g.euid, s); dev_free(g.out_rec, s);
+    dev_free(g.in_rec, s); dev_free(g.node_rng, s);
     delete h;
-    return cuda_fail(err, "cudaMalloc(device graph)");
+    return cuda_fail(err, "device graph allocation");
   }
-  (void)s;
+  g.stream = s;
   *out = h;
   return EVX_OK;
 }
 
 static int finish_graph(evx_graph *h, cudaStream_t s) {
   int *scratch = nullptr;
-  EVX_CUDA(cudaMalloc(&scratch, 2 * sizeof(int)));
+  EVX_CUDA(dev_alloc((void **)&scratch, 2 * sizeof(int), h->g.device, s));
   int rc = graph_t_range(h->g, scratch, s);
-  cudaFree(scratch);
+  dev_free(scratch, s);
   if (!rc) rc = build_pair_index(h->g, s);
   if (!rc) {
     EVX_CUDA(cudaStreamSynchronize(s));
@@ -209,9 +243,12 @@ int evx_graph_from_device(int device, int64_t num_edges, int64_t num_vertices, c
                           const int *out_v_d, const int *in_v_d, const int *out_r_d,
                           const int *in_r_d, const int *euid_d, void *stream, evx_graph **out) {
   cudaStream_t s = (cudaStream_t)stream;
+  if (!out || (num_edges > 0 && (!eg_d || !out_v_d || !in_v_d)) || !out_r_d || !in_r_d)
+    return fail(EVX_ERR_INVALID, "null graph array");
   int rc = alloc_graph(device, num_edges, num_vertices, out, s);
   if (rc) return rc;
-  rc = pack_graph((*out)->g, eg_d, out_v_d, in_v_d, out_r_d, in_r_d, euid_d, s);
+  rc = validate_graph(device, num_edges, num_vertices, eg_d, out_v_d, in_v_d, out_r_d, in_r_d, s);
+  if (!rc) rc = pack_graph((*out)->g, eg_d, out_v_d, in_v_d, out_r_d, in_r_d, euid_d, s);
   if (!rc) rc = finish_graph(*out, s);
   if (rc) { evx_graph_free(*out); *out = nullptr; }
   return rc;
@@ -223,36 +260,18 @@ int evx_graph_upload(int device, int64_t num_edges, int64_t num_vertices, const 
   if (!out || (num_edges > 0 && (!eg || !out_v || !in_v)) || !out_r || !in_r)
     return fail(EVX_ERR_INVALID, "null graph array");
   cudaStream_t s = (cudaStream_t)stream;
-  {
-    // The packing kernels index with these arrays: reject anything that
-    // would send them out of bounds.
-    const int64_t E = num_edges, V = num_vertices;
-    if (E < 0 || V < 0) return fail(EVX_ERR_INVALID, "negative sizes");
-    if (out_r[0] != 0 || in_r[0] != 0 || out_r[V] != E || in_r[V] != E)
-      return fail(EVX_ERR_INVALID, "CSR offsets must start at 0 and end at num_edges");
-    for (int64_t x = 0; x < V; x++)
-      if (out_r[x + 1] < out_r[x] || in_r[x + 1] < in_r[x])
-        return fail(EVX_ERR_INVALID, "CSR offsets are not monotone");
-    for (int64_t i = 0; i < E; i++) {
-      if ((unsigned)out_v[i] >= (uint64_t)E || (unsigned)in_v[i] >= (uint64_t)E)
-        return fail(EVX_ERR_INVALID, "edge id out of range in out/in lists");
-      if ((unsigned)eg[3 * i] >= (uint64_t)V || (unsigned)eg[3 * i + 1] >= (uint64_t)V)
-        return fail(EVX_ERR_INVALID, "vertex id out of range in Eg");
-      if (i && eg[3 * i + 2] < eg[3 * i - 1])
-        return fail(EVX_ERR_INVALID, "edges are not sorted by timestamp");
-    }
-  }
+  if (num_edges < 0 || num_vertices < 0) return fail(EVX_ERR_INVALID, "negative sizes");
   int rc = alloc_graph(device, num_edges, num_vertices, out, s);
   if (rc) return rc;
   const size_t E = (size_t)(num_edges > 0 ? num_edges : 1), V1 = (size_t)num_vertices + 1;
-  // staging in host-format layout (freed after packing)
+  // staging in host-format layout (returned to the pool after packing)
   int *buf = nullptr;
   const size_t n_ints = 3 * E + E + E + V1 + V1 + E;
-  cudaError_t err = cudaMalloc(&buf, n_ints * sizeof(int));
+  cudaError_t err = dev_alloc((void **)&buf, n_ints * sizeof(int), device, s);
   if (err != cudaSuccess) {
     evx_graph_free(*out);
     *out = nullptr;
-    return cuda_fail(err, "cudaMalloc(upload staging)");
+    return cuda_fail(err, "upload staging allocation");
   }
   int *eg_d = buf, *ov_d = eg_d + 3 * E, *iv_d = ov_d + E, *or_d = iv_d + E, *ir_d = or_d + V1,
       *eu_d = ir_d + V1;
@@ -270,10 +289,12 @@ int evx_graph_upload(int device, int64_t num_edges, int64_t num_vertices, const 
   C(or_d, out_r, sizeof(int) * V1);
   C(ir_d, in_r, sizeof(int) * V1);
   if (euid) C(eu_d, euid, sizeof(int) * ne);
+  // the packing kernels index with these arrays: check them on the device first
+  if (!rc) rc = validate_graph(device, num_edges, num_vertices, eg_d, ov_d, iv_d, or_d, ir_d, s);
   if (!rc) rc = pack_graph((*out)->g, eg_d, ov_d, iv_d, or_d, ir_d, euid ? eu_d : nullptr, s);
+  dev_free(buf, s);
   if (!rc) rc = finish_graph(*out, s);
   cudaStreamSynchronize(s);
-  cudaFree(buf);
   if (rc) { evx_graph_free(*out); *out = nullptr; }
   return rc;
 }
@@ -282,9 +303,14 @@ int evx_graph_free(evx_graph *h) {
   if (!h) return EVX_OK;
   DeviceGraph &g = h->g;
   cudaSetDevice(g.device);
-  cudaFree(g.edges); cudaFree(g.inpos); cudaFree(g.euid); cudaFree(g.out_rec);
-  cudaFree(g.in_rec); cudaFree(g.node_rng); cudaFree(g.pair_tab); cudaFree(g.pair_rec);
-  cudaFree(g.pair_loc);
+  // like cudaFree, wait for work that may still read the graph, then return
+  // its memory to the pool
+  cudaDeviceSynchronize();
+  cudaStream_t s = nullptr;  // the allocating stream may be gone; nothing is in flight now
+  dev_free(g.edges, s); dev_free(g.inpos, s); dev_free(g.euid, s); dev_free(g.out_rec, s);
+  dev_free(g.in_rec, s); dev_free(g.node_rng, s); dev_free(g.pair_tab, s); dev_free(g.pair_rec, s);
+  dev_free(g.pair_loc, s); dev_free(g.pair_dir, s); dev_free(g.dir_off, s);
+  cudaStreamSynchronize(s);
   delete h;
   return EVX_OK;
 }

@@ -53,6 +53,25 @@ __global__ void pack_nodes_kernel(const int *__restrict__ out_r, const int *__re
   }
 }
 
+// Input checks: edge ids in [0, E), vertex ids in [0, V), timestamps sorted,
+// CSR offsets monotone from 0 to E.  Bits of *err name the failed check.
+__global__ void validate_kernel(const int *__restrict__ eg, const int *__restrict__ out_v,
+                                const int *__restrict__ in_v, const int *__restrict__ out_r,
+                                const int *__restrict__ in_r, int E, int V, int *err) {
+  const int n = max(E, V + 1);
+  int bad = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (i < E) {
+      if ((unsigned)out_v[i] >= (unsigned)E || (unsigned)in_v[i] >= (unsigned)E) bad |= 1;
+      if ((unsigned)eg[3 * i] >= (unsigned)V || (unsigned)eg[3 * i + 1] >= (unsigned)V) bad |= 2;
+      if (i > 0 && eg[3 * i + 2] < eg[3 * i - 1]) bad |= 4;
+    }
+    if (i < V && (out_r[i + 1] < out_r[i] || in_r[i + 1] < in_r[i])) bad |= 8;
+    if (i == 0 && (out_r[0] != 0 || in_r[0] != 0 || out_r[V] != E || in_r[V] != E)) bad |= 16;
+  }
+  if (bad) atomicOr(err, bad);
+}
+
 // min / max timestamp (for the t + delta overflow check)
 __global__ void t_range_kernel(const int4 *__restrict__ edges, int n, int *out) {
   int lo = INT_MAX, hi = INT_MIN;
@@ -87,14 +106,36 @@ int pack_graph(DeviceGraph &g, const int *eg_d, const int *out_v_d, const int *i
   if (V > 0) pack_nodes_kernel<<<grid, block, 0, s>>>(out_r_d, in_r_d, g.node_rng, (int)V);
   if (E > 0) {
     int *outpos = nullptr;  // edges[].w, staged
-    EVX_CUDA(cudaMallocAsync(&outpos, sizeof(int) * (size_t)E, s));
+    EVX_CUDA(dev_alloc((void **)&outpos, sizeof(int) * (size_t)E, g.device, s));
     scatter_pos_kernel<<<grid, block, 0, s>>>(out_v_d, in_v_d, outpos, g.inpos, (int)E);
     pack_edges_kernel<<<grid, block, 0, s>>>(eg_d, euid_d, outpos, g.edges, g.euid, (int)E);
     pack_rec_kernel<<<grid, block, 0, s>>>(out_v_d, in_v_d, g.edges, g.inpos, g.out_rec, g.in_rec,
                                            (int)E);
-    EVX_CUDA(cudaFreeAsync(outpos, s));
+    dev_free(outpos, s);
   }
   EVX_CUDA(cudaGetLastError());
+  return EVX_OK;
+}
+
+int validate_graph(int device, int64_t E, int64_t V, const int *eg_d, const int *out_v_d, const int *in_v_d,
+                   const int *out_r_d, const int *in_r_d, cudaStream_t s) {
+  int *err = nullptr;
+  EVX_CUDA(dev_alloc((void **)&err, sizeof(int), device, s));
+  EVX_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  validate_kernel<<<sms * 8, 256, 0, s>>>(eg_d, out_v_d, in_v_d, out_r_d, in_r_d, (int)E, (int)V, err);
+  int h = 0;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  dev_free(err, s);
+  if (e != cudaSuccess) return cuda_fail(e, "graph validation");
+  if (h & 1) return fail(EVX_ERR_INVALID, "edge id out of range in out/in lists");
+  if (h & 2) return fail(EVX_ERR_INVALID, "vertex id out of range in Eg");
+  if (h & 4) return fail(EVX_ERR_INVALID, "edges are not sorted by timestamp");
+  if (h & 8) return fail(EVX_ERR_INVALID, "CSR offsets are not monotone");
+  if (h & 16) return fail(EVX_ERR_INVALID, "CSR offsets must start at 0 and end at num_edges");
   return EVX_OK;
 }
 

@@ -30,6 +30,8 @@ struct GraphView {
   const int4 *pair_tab;
   const int2 *pair_rec;
   const int2 *pair_loc;       // [e] = {position of e in pair_rec, end of its run}
+  const int2 *pair_dir;       // [r] = {v, start} of run r, sorted by (u, v); [P] = sentinel
+  const int *dir_off;         // [u] = first run of source u (V + 1 entries)
   unsigned long long pair_mask;
   int pair_max_probe;
   int num_edges;
@@ -71,6 +73,7 @@ __host__ __device__ inline int plan_nm(int w) { return (w >> 12) & 15; }
 constexpr int kQStrict = 1;      // t(e_j) > t(e_{j-1}) as well
 constexpr int kQInlineLast = 2;  // closing last edge counted on the pair index
 constexpr int kQSamePair = 4;    // last edge repeats the previous edge's endpoints
+constexpr int kQPairDir = 8;     // last edge's pair found through the per-node pair directory
 struct QueryDesc {
   MotifPlan plan;
   int root_beg, root_end;  // root edge ids [beg, end)
@@ -122,6 +125,7 @@ struct SearchArgs {
 // Host-side graph object.
 struct DeviceGraph {
   int device = 0;
+  cudaStream_t stream = nullptr;  // stream its memory was allocated on
   int64_t num_edges = 0, num_vertices = 0;
   int max_t = 0, min_t = 0;
   int4 *edges = nullptr;
@@ -133,6 +137,8 @@ struct DeviceGraph {
   int4 *pair_tab = nullptr;
   int2 *pair_rec = nullptr;
   int2 *pair_loc = nullptr;
+  int2 *pair_dir = nullptr;
+  int *dir_off = nullptr;
   unsigned long long pair_mask = 0;
   int pair_max_probe = 0;
   int64_t bytes = 0;
@@ -141,6 +147,7 @@ struct DeviceGraph {
     g.edges = edges; g.inpos = inpos; g.euid = euid; g.out_rec = out_rec; g.in_rec = in_rec;
     g.node_rng = node_rng;
     g.pair_tab = pair_tab; g.pair_rec = pair_rec; g.pair_loc = pair_loc; g.pair_mask = pair_mask;
+    g.pair_dir = pair_dir; g.dir_off = dir_off;
     g.pair_max_probe = pair_max_probe;
     g.num_edges = (int)num_edges; g.num_vertices = (int)num_vertices;
     return g;
@@ -151,6 +158,12 @@ struct DeviceGraph {
 int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan);
 // How a count query counts its last edge (kQInlineLast, kQSamePair or 0).
 int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate);
+
+// Stream-ordered device allocations from a library-owned pool per device
+// that keeps freed memory mapped (graph re-uploads and pair-index scratch
+// reuse it instead of paying for fresh cudaMalloc / cudaFree each time).
+cudaError_t dev_alloc(void **p, size_t bytes, int device, cudaStream_t s);
+void dev_free(void *p, cudaStream_t s);
 
 // Error plumbing (thread-local message).
 void set_error(const std::string &msg);
@@ -176,6 +189,11 @@ int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm);
 
 // Build the pair index (defined in evx_pairs.cu); needs edges[] packed.
 int build_pair_index(DeviceGraph &g, cudaStream_t s);
+
+// Check the host-format arrays on the device before anything indexes with
+// them (evx_graph.cu); returns EVX_ERR_INVALID with a message on bad input.
+int validate_graph(int device, int64_t E, int64_t V, const int *eg_d, const int *out_v_d, const int *in_v_d,
+                   const int *out_r_d, const int *in_r_d, cudaStream_t s);
 
 // Build the packed device layout from the uploaded host-format arrays
 // (defined in evx_graph.cu).

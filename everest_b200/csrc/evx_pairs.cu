@@ -44,6 +44,23 @@ __global__ void pair_loc_kernel(const int *__restrict__ eids, const int *__restr
   }
 }
 
+// dir[r] = {v, start} of run r (runs sorted by (u, v)); dir[P] = sentinel;
+// node_cnt[u] = runs of source u
+__global__ void pair_dir_kernel(const unsigned long long *__restrict__ ukeys,
+                                const int *__restrict__ starts, const int *__restrict__ num_runs,
+                                int2 *__restrict__ dir, int *__restrict__ node_cnt, int n_edges) {
+  const int P = *num_runs;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r <= P; r += gridDim.x * blockDim.x) {
+    if (r == P) {
+      dir[r] = make_int2(0x7fffffff, n_edges);
+    } else {
+      const unsigned long long k = ukeys[r];
+      dir[r] = make_int2((int)(unsigned)(k & 0xffffffffull), starts[r]);
+      atomicAdd(node_cnt + (int)(k >> 32), 1);
+    }
+  }
+}
+
 __global__ void pair_clear_kernel(int4 *__restrict__ tab, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -85,11 +102,19 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
   if (E <= 0) {
     g.pair_mask = 0;
     g.pair_max_probe = 0;
-    EVX_CUDA(cudaMalloc(&g.pair_tab, sizeof(int4)));
-    EVX_CUDA(cudaMalloc(&g.pair_rec, sizeof(int2)));
-    EVX_CUDA(cudaMalloc(&g.pair_loc, sizeof(int2)));
+    EVX_CUDA(dev_alloc((void **)&g.pair_tab, sizeof(int4), g.device, s));
+    EVX_CUDA(dev_alloc((void **)&g.pair_rec, sizeof(int2), g.device, s));
+    EVX_CUDA(dev_alloc((void **)&g.pair_loc, sizeof(int2), g.device, s));
+    EVX_CUDA(dev_alloc((void **)&g.pair_dir, sizeof(int2), g.device, s));
+    EVX_CUDA(dev_alloc((void **)&g.dir_off, sizeof(int) * (size_t)(g.num_vertices + 1), g.device, s));
     EVX_CUDA(cudaMemsetAsync(g.pair_tab, 0xff, sizeof(int4), s));
-    g.bytes += sizeof(int4) + 2 * sizeof(int2);
+    EVX_CUDA(cudaMemsetAsync(g.dir_off, 0, sizeof(int) * (size_t)(g.num_vertices + 1), s));
+    {
+      const int2 sentinel = make_int2(0x7fffffff, 0);
+      EVX_CUDA(cudaMemcpyAsync(g.pair_dir, &sentinel, sizeof(int2), cudaMemcpyHostToDevice, s));
+      EVX_CUDA(cudaStreamSynchronize(s));
+    }
+    g.bytes += sizeof(int4) + 3 * sizeof(int2) + sizeof(int) * (g.num_vertices + 1);
     return EVX_OK;
   }
   int sms = 148;
@@ -103,7 +128,7 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
   int rc = EVX_OK;
   auto A = [&](void **p, size_t b) {
     if (rc == EVX_OK) {
-      cudaError_t e = cudaMallocAsync(p, b, s);
+      cudaError_t e = dev_alloc(p, b, g.device, s);
       if (e != cudaSuccess) rc = cuda_fail(e, "cudaMallocAsync(pair index scratch)");
     }
   };
@@ -143,9 +168,9 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     long long cap = 1;
     while (cap < 2ll * runs + 2) cap <<= 1;
     g.pair_mask = (unsigned long long)(cap - 1);
-    cudaError_t e = cudaMalloc(&g.pair_tab, sizeof(int4) * (size_t)cap);
-    if (e == cudaSuccess) e = cudaMalloc(&g.pair_rec, sizeof(int2) * (size_t)n);
-    if (e == cudaSuccess) e = cudaMalloc(&g.pair_loc, sizeof(int2) * (size_t)n);
+    cudaError_t e = dev_alloc((void **)&g.pair_tab, sizeof(int4) * (size_t)cap, g.device, s);
+    if (e == cudaSuccess) e = dev_alloc((void **)&g.pair_rec, sizeof(int2) * (size_t)n, g.device, s);
+    if (e == cudaSuccess) e = dev_alloc((void **)&g.pair_loc, sizeof(int2) * (size_t)n, g.device, s);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMalloc(pair index)"); goto cleanup; }
     g.bytes += (int64_t)(sizeof(int4) * cap + 2 * sizeof(int2) * n);
     EVX_CUDA(cudaMemsetAsync(ctr + 1, 0, 2 * sizeof(int), s));
@@ -154,6 +179,30 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     pair_loc_kernel<<<grid, block, 0, s>>>(vals_sorted, starts, lens, ctr, g.pair_loc);
     pair_insert_kernel<<<grid, block, 0, s>>>(ukeys, starts, lens, ctr, g.pair_tab, g.pair_mask, ctr + 1,
                                               ctr + 2);
+    // per-node directory of distinct out-neighbours (sorted) -> pair runs
+    {
+      const int64_t V = g.num_vertices;
+      cudaError_t e2 = dev_alloc((void **)&g.pair_dir, sizeof(int2) * ((size_t)runs + 1), g.device, s);
+      if (e2 == cudaSuccess) e2 = dev_alloc((void **)&g.dir_off, sizeof(int) * (size_t)(V + 1), g.device, s);
+      if (e2 != cudaSuccess) { rc = cuda_fail(e2, "cudaMalloc(pair directory)"); goto cleanup; }
+      g.bytes += (int64_t)(sizeof(int2) * ((size_t)runs + 1) + sizeof(int) * (V + 1));
+      int *node_cnt = nullptr;
+      A((void **)&node_cnt, sizeof(int) * (size_t)(V + 1));
+      if (rc) goto cleanup;
+      EVX_CUDA(cudaMemsetAsync(node_cnt, 0, sizeof(int) * (size_t)(V + 1), s));
+      pair_dir_kernel<<<grid, block, 0, s>>>(ukeys, starts, ctr, g.pair_dir, node_cnt, n);
+      size_t t4 = 0;
+      cub::DeviceScan::ExclusiveSum(nullptr, t4, node_cnt, g.dir_off, (int)(V + 1), s);
+      if (t4 > tmp_bytes) {
+        dev_free(tmp, s);
+        tmp = nullptr;
+        A(&tmp, t4);
+        if (rc) goto cleanup;
+        tmp_bytes = t4;
+      }
+      cub::DeviceScan::ExclusiveSum(tmp, t4, node_cnt, g.dir_off, (int)(V + 1), s);
+      dev_free(node_cnt, s);
+    }
     int h[2] = {0, 0};
     EVX_CUDA(cudaGetLastError());
     EVX_CUDA(cudaMemcpyAsync(h, ctr + 1, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -162,15 +211,15 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     g.pair_max_probe = h[0];
   }
 cleanup:
-  cudaFreeAsync(keys, s);
-  cudaFreeAsync(keys_sorted, s);
-  cudaFreeAsync(ukeys, s);
-  cudaFreeAsync(vals, s);
-  cudaFreeAsync(vals_sorted, s);
-  cudaFreeAsync(lens, s);
-  cudaFreeAsync(starts, s);
-  cudaFreeAsync(ctr, s);
-  if (tmp) cudaFreeAsync(tmp, s);
+  dev_free(keys, s);
+  dev_free(keys_sorted, s);
+  dev_free(ukeys, s);
+  dev_free(vals, s);
+  dev_free(vals_sorted, s);
+  dev_free(lens, s);
+  dev_free(starts, s);
+  dev_free(ctr, s);
+  dev_free(tmp, s);
   if (rc == EVX_OK) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) rc = cuda_fail(e, "pair index build");

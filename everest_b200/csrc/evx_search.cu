@@ -46,7 +46,10 @@ constexpr int kBlock = 128;     // threads per block
 constexpr int kWarps = kBlock / 32;
 // resident blocks per SM the register budget aims for (deeper motifs keep
 // more per-level state live)
-constexpr int min_blocks(int k) { return k <= 3 ? 8 : (k == 4 ? 6 : 4); }
+#ifndef EVX_MINB3
+#define EVX_MINB3 8
+#endif
+constexpr int min_blocks(int k) { return k <= 3 ? EVX_MINB3 : (k == 4 ? 6 : 4); }
 
 template <int N>
 __device__ __forceinline__ int sel(const int (&a)[N], int i) {
@@ -99,6 +102,12 @@ __device__ __forceinline__ int pair_first_t_after(const GraphView &g, int lo, in
   return lo;
 }
 
+// Count of u->v edges after the previous edge (id > key; t > key in strict
+// mode) inside the window, through u's sorted directory of distinct
+// out-neighbours.
+__device__ __forceinline__ int pair_dir_window(const GraphView &g, int u, int v, int key, int tl,
+                                               bool strict);
+
 // Same, galloping up from lo (windows are usually a few entries long).
 __device__ __forceinline__ int pair_gallop_t_after(const GraphView &g, int lo, int hi, int tl) {
   int step = 1;
@@ -121,6 +130,20 @@ __device__ __forceinline__ int pair_first_key_after(const GraphView &g, int lo, 
     if ((strict ? r.y : r.x) > key) hi = mid; else lo = mid + 1;
   }
   return lo;
+}
+
+__device__ __forceinline__ int pair_dir_window(const GraphView &g, int u, int v, int key, int tl,
+                                               bool strict) {
+  int lo = __ldg(g.dir_off + u), hi = __ldg(g.dir_off + u + 1);
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(&g.pair_dir[mid].x) < v) lo = mid + 1; else hi = mid;
+  }
+  const int2 d0 = __ldg(g.pair_dir + lo);
+  if (d0.x != v || lo >= __ldg(g.dir_off + u + 1)) return 0;
+  const int stop = __ldg(&g.pair_dir[lo + 1].y);
+  const int a = pair_first_key_after(g, d0.y, stop, key, strict);
+  return pair_gallop_t_after(g, a, stop, tl) - a;
 }
 
 // Entries of the run [start, start + len) after the previous edge (edge id >
@@ -186,7 +209,7 @@ struct Searcher {
   const int lane;
   const unsigned lt;
   // the current query's options (reloaded when the warp switches queries)
-  int strict = 0, inline_last = 0, same_pair = 0, steal_interval = 0, min_split = 2, kq = K;
+  int strict = 0, inline_last = 0, same_pair = 0, pair_dir = 0, steal_interval = 0, min_split = 2, kq = K;
   // motif edges of the current query: K itself when the launch has one
   // motif size (EXACT), else the table entry's
   __device__ __forceinline__ int kr() const { return EXACT ? K : kq; }
@@ -200,6 +223,7 @@ struct Searcher {
     strict = (q.flags & kQStrict) ? 1 : 0;
     inline_last = (q.flags & kQInlineLast) ? 1 : 0;
     same_pair = (q.flags & kQSamePair) ? 1 : 0;
+    pair_dir = (q.flags & kQPairDir) ? 1 : 0;
     steal_interval = q.steal_interval;
     min_split = q.min_split;
     kq = q.plan.k;
@@ -308,6 +332,19 @@ struct Searcher {
       }
     }
     int tl = sm.root[root].z;
+
+    // --------------------------- last level through the pair directory ----
+    if (!ENUM && pair_dir && l == kr() - 2) {
+      // the closing last edge of each lane's task: count its static pair's
+      // run inside the window (converged across the batch's 32 tasks)
+      if (has) {
+        const int w = plan.info[l];
+        const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
+        const int tlc = sm.root[root].z;
+        cnt += (unsigned long long)pair_dir_window(g, ia, ib, strict ? p.t : p.eid, tlc, strict != 0);
+      }
+      return;
+    }
 
     // ------------------------------------------------------- open list ----
     const int w = plan.info[l];
@@ -633,6 +670,11 @@ int setup_k() {
     cudaError_t e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(kWarps * sizeof(WarpSmem<K>)));
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+#ifdef EVX_CARVEOUT
+    e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             EVX_CARVEOUT);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(carveout)");
+#endif
     done = true;
   }
   return 0;

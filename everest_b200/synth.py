@@ -20,10 +20,13 @@ Graph families
            follow a power law with exponent ``alpha``), a start time uniform
            in ``[0, t_span)``, a size ``max(1, Poisson(burst_mean))`` and
            exponential inter-edge gaps of mean ``gap_mean`` seconds.  Each
-           edge of the burst draws its destination from an independent power
-           law weighting (its own permutation, same exponent); a destination
-           equal to the source is redrawn.  Bursts are generated until ``E``
-           edges exist, then truncated to exactly ``E``.
+           edge of the burst draws its destination independently from a power
+           law over the same node ranking (nodes that send much also receive
+           much, as in message graphs); a destination equal to the source is
+           redrawn.  With probability ``reply`` an edge after the first is a
+           reply instead: it goes from the destination of the burst's latest
+           non-reply edge back to the burst's source.  Bursts are generated until ``E`` edges
+           exist, then truncated to exactly ``E``.
 """
 from __future__ import annotations
 
@@ -53,6 +56,7 @@ class GraphSpec:
     t_span: int = 230_000_000    # bursty family: burst starts ~ U[0, t_span)
     burst_mean: float = 20.0     # bursty family: Poisson mean burst size
     gap_mean: float = 60.0       # bursty family: mean intra-burst gap (s)
+    reply: float = 0.25          # bursty family: probability an edge answers the burst source
 
 
 SPECS: Dict[str, GraphSpec] = {
@@ -97,8 +101,7 @@ def _gen_zipf(spec: GraphSpec, rng: np.random.Generator):
 def _gen_bursty(spec: GraphSpec, rng: np.random.Generator):
     V, E = spec.num_nodes, spec.num_edges
     s = 1.0 / (spec.alpha - 1.0)
-    perm_src = rng.permutation(V).astype(np.int32)
-    perm_dst = rng.permutation(V).astype(np.int32)
+    perm = rng.permutation(V).astype(np.int32)
     draw_src = _zipf_sampler(rng, V, s)
     draw_dst = _zipf_sampler(rng, V, s)
     # enough bursts for E edges (mean size >= burst_mean for Poisson clipped at 1)
@@ -120,16 +123,23 @@ def _gen_bursty(spec: GraphSpec, rng: np.random.Generator):
     cg = np.cumsum(gaps)
     base = cg[first] - gaps[first]           # cumulative gap before the burst's first edge
     t = np.floor(starts[burst_of] + (cg - base[burst_of])).astype(np.int64)
-    src = burst_src[burst_of]
-    dst = draw_dst(E)
-    s_ids = perm_src[src]
-    d_ids = perm_dst[dst]
+    s_ids = perm[burst_src[burst_of]]
+    d_ids = perm[draw_dst(E)]
     bad = s_ids == d_ids
     while bad.any():
         k = int(bad.sum())
-        d_ids[bad] = perm_dst[draw_dst(k)]
+        d_ids[bad] = perm[draw_dst(k)]
         bad = s_ids == d_ids
-    return s_ids, d_ids, t
+    # replies: edge i (not the first of its burst) answers the burst source
+    # from the destination of the burst's latest non-reply edge
+    idx = np.arange(E, dtype=np.int64)
+    pos_in_burst = idx - first[burst_of]
+    rep = (rng.random(E) < spec.reply) & (pos_in_burst > 0)
+    last_plain = np.maximum.accumulate(np.where(rep, -1, idx))  # first edge of a burst is plain
+    src_out, dst_out = s_ids.copy(), d_ids.copy()
+    src_out[rep] = d_ids[last_plain[rep]]
+    dst_out[rep] = s_ids[rep]
+    return src_out, dst_out, t
 
 
 def generate(spec: GraphSpec) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:

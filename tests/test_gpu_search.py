@@ -58,6 +58,10 @@ def test_golden_small_graph_counts(golden, small_graphs, worker):
             rb, re_ = c.get("roots", [0, -1])
             got = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_)
             assert got == c["count"], (gname, c["motif"], c["delta"], got, c["count"])
+            if n % 5 == 0:  # the directory-counted last level on a subset
+                got3 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
+                                 flags=capi.FLAG_PAIR_DIR)
+                assert got3 == c["count"], (gname, c["motif"], c["delta"], got3, "pair dir")
             if n % 7 == 0:  # the scanning last level on a subset
                 got2 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
                                  flags=capi.FLAG_NO_PAIR_INDEX)
@@ -89,6 +93,8 @@ def test_golden_zipf_200k(golden, worker):
         assert gpu_count(worker, dg, p["mu"], p["mv"], p["delta"],
                          flags=capi.FLAG_NO_PAIR_INDEX) == p["count"], p["motif"]
         assert gpu_count(worker, dg, p["mu"], p["mv"], p["delta"],
+                         flags=capi.FLAG_PAIR_DIR) == p["count"], p["motif"]
+        assert gpu_count(worker, dg, p["mu"], p["mv"], p["delta"],
                          flags=capi.FLAG_STRICT_TS) == gpu_count(
             worker, dg, p["mu"], p["mv"], p["delta"],
             flags=capi.FLAG_STRICT_TS | capi.FLAG_NO_PAIR_INDEX), p["motif"]
@@ -110,7 +116,7 @@ def test_random_tiny_vs_brute_force(worker):
         delta = int(rng.integers(0, 10))
         want = len(O.brute_force(u, v, t, mu, mv, delta))
         dg = device_graph(u, v, t)
-        for flags in (0, capi.FLAG_NO_STEAL, capi.FLAG_NO_PAIR_INDEX):
+        for flags in (0, capi.FLAG_NO_STEAL, capi.FLAG_NO_PAIR_INDEX, capi.FLAG_PAIR_DIR):
             assert gpu_count(worker, dg, mu, mv, delta, flags=flags) == want, (trial, pat, delta, flags)
         strict = len(O.brute_force(u, v, t, mu, mv, delta, strict_ts=True))
         assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS) == strict
