@@ -56,6 +56,16 @@ def parse():
     ap.add_argument("--single-query", type=int, default=-1,
                     help="profiling aid: run only query I of the workload --reps times and exit")
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--mode", default="single", choices=["single", "batch", "serve"],
+                    help="single: the 36-query per-query-kernel step (default); batch: one persistent "
+                         "launch of 64 mixed queries vs the same queries one at a time; serve: the "
+                         "serving loop under Poisson arrivals vs one at a time")
+    ap.add_argument("--queries", type=int, default=0, help="batch/serve: number of queries")
+    ap.add_argument("--window", type=int, default=0,
+                    help="batch/serve: roots per query (a random time window of the edge list)")
+    ap.add_argument("--limit", type=float, default=1e9,
+                    help="batch/serve: work limit per query, in adjacency records examined inside "
+                         "their time windows (stopped queries are flagged in both arms)")
     return ap.parse_args()
 
 
@@ -287,6 +297,7 @@ def run_gpu_arm(args):
     with ClockSampler(dev) as clk:
         for _ in range(args.steps):
             ms, counts, kms, nl = device_step()
+            per_query_ms = {q["name"]: round(w.last_stats()["device_ms"], 3) for q, w in zip(qs, workers)}
             step_ms.append(ms)
             kern_ms.append(kms)
             launches += nl
@@ -346,6 +357,7 @@ def run_gpu_arm(args):
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e_total / args.steps},
         "gpu_launches": launches,
+        "per_query_ms": per_query_ms,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs",
@@ -394,6 +406,9 @@ def main():
     args = parse()
     if args.single_query >= 0:
         return run_single_query(args)
+    if args.mode in ("batch", "serve"):
+        from everest_b200 import bench_modes
+        return bench_modes.run(args)
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_gpu_arm(args)

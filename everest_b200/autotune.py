@@ -124,15 +124,18 @@ class Autotuner:
         finally:
             self.apply(worker, DEFAULT)
 
-    def tune_batch(self, batch_factory, queries, graph: capi.DeviceGraph) -> int:
-        """Pick the tile size for a batch of (mu, mv, delta) queries; returns
-        tile_roots (the batch's counts must not depend on it: checked)."""
+    def tune_batch(self, batch_factory, queries, graph: capi.DeviceGraph, limit: int = 0) -> int:
+        """Pick the tile size for a batch of (mu, mv, delta[, beg, end])
+        queries; returns tile_roots (the batch's counts must not depend on
+        it: checked; with a work limit the stopped queries must match too)."""
         best, best_ms, ref = BATCH_TILES[0], float("inf"), None
         for tr in BATCH_TILES:
             b = batch_factory()
             b.set_tuning(tile_roots=tr)
-            for mu, mv, d in queries:
-                b.add(graph, mu, mv, d)
+            if limit:
+                b.set_limit(limit)
+            for q in queries:
+                b.add(graph, *q)
             r = b.run()
             r = b.run()
             ms = b.last_stats()["device_ms"]

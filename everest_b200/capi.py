@@ -19,7 +19,10 @@ EVX_OK = 0
 EVX_ERR = {
     -1: "EVX_ERR_INVALID", -2: "EVX_ERR_CUDA", -3: "EVX_ERR_NOMEM", -4: "EVX_ERR_OVERFLOW",
     -5: "EVX_ERR_IO", -6: "EVX_ERR_STATE", -7: "EVX_ERR_TIMEOUT", -8: "EVX_ERR_NODEVICE",
+    -9: "EVX_ERR_LIMIT",
 }
+EVX_ERR_LIMIT = -9
+LIMITED = 2**64 - 1  # Batch.result() count of a query stopped at the work limit
 FLAG_STRICT_TS = 1
 FLAG_EXACT_TOTAL = 2
 FLAG_NO_STEAL = 4
@@ -37,7 +40,8 @@ EXPORTS = [
     "evx_worker_last_stats", "evx_host_register", "evx_host_unregister", "evx_count_static",
     "evx_batch_create", "evx_batch_destroy", "evx_batch_add", "evx_batch_clear", "evx_batch_launch",
     "evx_batch_result", "evx_batch_run", "evx_batch_set_tuning", "evx_batch_last_stats",
-    "evx_device_mem_info", "evx_worker_query", "evx_batch_query",
+    "evx_device_mem_info", "evx_worker_query", "evx_batch_query", "evx_worker_set_limit",
+    "evx_batch_set_limit",
 ]
 STATIC_MAX_QUERIES = 256
 
@@ -46,6 +50,16 @@ class EvxError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"{EVX_ERR.get(code, code)}: {msg}")
         self.code = code
+
+
+class LimitExceeded(EvxError):
+    """A query passed its work limit; ``count`` is the lower bound counted
+    before the search stopped."""
+
+    def __init__(self, count: int, limit: int):
+        super().__init__(EVX_ERR_LIMIT, f"work limit {limit} exceeded (counted {count} before stopping)")
+        self.count = count
+        self.limit = limit
 
 
 _lib = None
@@ -95,6 +109,8 @@ def lib():
             "evx_worker_result": ([_P, _PU64], _I),
             "evx_worker_enum_rows": ([_P, _I64, _P, _PI64], _I),
             "evx_worker_set_tuning": ([_P, _I, _I, _I, _I, _I], _I),
+            "evx_worker_set_limit": ([_P, ctypes.c_uint64], _I),
+            "evx_batch_set_limit": ([_P, ctypes.c_uint64], _I),
             "evx_worker_last_stats": ([_P, _PI, ctypes.POINTER(ctypes.c_float)], _I),
             "evx_batch_create": ([_I, _I, _P, ctypes.POINTER(_P)], _I),
             "evx_batch_destroy": ([_P], _I),
@@ -357,18 +373,29 @@ class Worker:
         self.k = k
         self.enum_cap = int(enum_cap)
 
+    def set_limit(self, max_work: int) -> None:
+        """Work limit of later jobs (0 = none), in adjacency records examined
+        inside their time windows; run()/result() raise LimitExceeded for a
+        query whose work passes it (an enumeration keeps its rows so far)."""
+        check(lib().evx_worker_set_limit(self._h, int(max_work)))
+        self.limit = int(max_work)
+
+    def _count(self, rc: int, c: ctypes.c_uint64) -> int:
+        if rc == EVX_ERR_LIMIT:
+            raise LimitExceeded(int(c.value), getattr(self, "limit", 0))
+        check(rc)
+        return int(c.value)
+
     def run(self) -> int:
         c = ctypes.c_uint64(0)
-        check(lib().evx_worker_run(self._h, ctypes.byref(c)))
-        return int(c.value)
+        return self._count(lib().evx_worker_run(self._h, ctypes.byref(c)), c)
 
     def launch(self) -> None:
         check(lib().evx_worker_launch(self._h))
 
     def result(self) -> int:
         c = ctypes.c_uint64(0)
-        check(lib().evx_worker_result(self._h, ctypes.byref(c)))
-        return int(c.value)
+        return self._count(lib().evx_worker_result(self._h, ctypes.byref(c)), c)
 
     def done(self) -> bool:
         """True once the launched search has finished (never blocks)."""
@@ -416,6 +443,12 @@ class Batch:
     def set_tuning(self, tile_roots=256, blocks_per_sm=0, steal_interval=16, min_split=2, use_graph=True):
         check(lib().evx_batch_set_tuning(self._h, tile_roots, blocks_per_sm, steal_interval, min_split,
                                          1 if use_graph else 0, 0))
+
+    def set_limit(self, max_work: int) -> None:
+        """Work limit per query (0 = none); result() then holds LIMITED for
+        each query that was stopped."""
+        check(lib().evx_batch_set_limit(self._h, int(max_work)))
+        self.limit = int(max_work)
 
     def add(self, graph: DeviceGraph, mu, mv, delta, beg=0, end=-1, flags=0) -> int:
         k = len(mu)

@@ -9,6 +9,7 @@
 // reset, kernel, counts read-back) is captured once into a CUDA graph and
 // replayed while the batch keeps the same shape.
 #include <climits>
+#include <cstdint>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -27,14 +28,16 @@ struct evx_batch {
   std::vector<QueryDesc> queries;
   QueryDesc *table_d = nullptr;        // [max_q]
   QueryDesc *table_h = nullptr;        // pinned [max_q]
-  unsigned long long *counts_d = nullptr;  // [max_q] + cursor word
-  unsigned long long *counts_h = nullptr;  // pinned [max_q]
+  unsigned long long *counts_d = nullptr;  // [max_q] counts, cursor word, [max_q] work meters
+  unsigned long long *counts_h = nullptr;  // pinned [max_q] counts, [max_q] meters
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // tuning
   int tile_roots = 256, blocks_per_sm = 0, steal_interval = 16, min_split = 2, use_graph = 1;
+  unsigned long long limit = 0;  // work limit per query (0 = none)
   // captured launch and the shape it was captured for
   cudaGraphExec_t exec = nullptr;
   int exec_nq = -1, exec_kmax = -1, exec_tiles = -1, exec_grid = -1, exec_tile_roots = -1;
+  unsigned long long exec_limit = 0;
   const evx_graph *exec_graph = nullptr;
   bool launched = false;
   int last_launches = 0;
@@ -53,7 +56,7 @@ int enqueue(evx_batch *b, int nq, int kmax, int total_tiles, int grid) {
   int *cursor = reinterpret_cast<int *>(b->counts_d + b->max_q);
   EVX_CUDA(cudaMemcpyAsync(b->table_d, b->table_h, sizeof(QueryDesc) * (size_t)nq, cudaMemcpyHostToDevice,
                            b->stream));
-  EVX_CUDA(cudaMemsetAsync(b->counts_d, 0, sizeof(unsigned long long) * ((size_t)b->max_q + 1), b->stream));
+  EVX_CUDA(cudaMemsetAsync(b->counts_d, 0, sizeof(unsigned long long) * (2 * (size_t)b->max_q + 1), b->stream));
   LaunchArgs la;
   la.table = b->table_d;
   la.nq = nq;
@@ -61,6 +64,8 @@ int enqueue(evx_batch *b, int nq, int kmax, int total_tiles, int grid) {
   la.tile_roots = b->tile_roots;
   la.cursor = cursor;
   la.counts = b->counts_d;
+  la.limit = b->limit;
+  la.meter = b->counts_d + b->max_q + 1;
   if (total_tiles > 0) {
     int rc = launch_table(b->graph->g.view(), b->table_h[0], la, kmax, grid, b->stream);
     if (rc) return rc;
@@ -68,6 +73,9 @@ int enqueue(evx_batch *b, int nq, int kmax, int total_tiles, int grid) {
   }
   EVX_CUDA(cudaMemcpyAsync(b->counts_h, b->counts_d, sizeof(unsigned long long) * (size_t)nq,
                            cudaMemcpyDeviceToHost, b->stream));
+  if (b->limit)
+    EVX_CUDA(cudaMemcpyAsync(b->counts_h + b->max_q, la.meter, sizeof(unsigned long long) * (size_t)nq,
+                             cudaMemcpyDeviceToHost, b->stream));
   return EVX_OK;
 }
 
@@ -97,8 +105,8 @@ int evx_batch_create(int device, int max_queries, void *stream, evx_batch **out)
   }
   if (e == cudaSuccess) e = cudaMalloc(&b->table_d, sizeof(QueryDesc) * (size_t)max_queries);
   if (e == cudaSuccess) e = cudaMallocHost(&b->table_h, sizeof(QueryDesc) * (size_t)max_queries);
-  if (e == cudaSuccess) e = cudaMalloc(&b->counts_d, sizeof(unsigned long long) * ((size_t)max_queries + 1));
-  if (e == cudaSuccess) e = cudaMallocHost(&b->counts_h, sizeof(unsigned long long) * (size_t)max_queries);
+  if (e == cudaSuccess) e = cudaMalloc(&b->counts_d, sizeof(unsigned long long) * (2 * (size_t)max_queries + 1));
+  if (e == cudaSuccess) e = cudaMallocHost(&b->counts_h, sizeof(unsigned long long) * 2 * (size_t)max_queries);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
   if (e != cudaSuccess) {
@@ -148,6 +156,13 @@ int evx_batch_set_tuning(evx_batch *b, int tile_roots, int blocks_per_sm, int st
   b->min_split = min_split;
   b->use_graph = use_graph ? 1 : 0;
   drop_exec(b);
+  return EVX_OK;
+}
+
+int evx_batch_set_limit(evx_batch *b, uint64_t max_work) {
+  if (!b) return fail(EVX_ERR_INVALID, "null batch");
+  if (b->launched) return fail(EVX_ERR_STATE, "batch launched: read its result first");
+  b->limit = max_work;
   return EVX_OK;
 }
 
@@ -214,7 +229,8 @@ int evx_batch_launch(evx_batch *b) {
   EVX_CUDA(cudaEventRecord(b->ev0, b->stream));
   if (b->use_graph) {
     if (!b->exec || b->exec_nq != nq || b->exec_kmax != kmax || b->exec_tiles != tiles ||
-        b->exec_grid != grid || b->exec_tile_roots != b->tile_roots || b->exec_graph != b->graph) {
+        b->exec_grid != grid || b->exec_tile_roots != b->tile_roots || b->exec_graph != b->graph ||
+        b->exec_limit != b->limit) {
       drop_exec(b);
       cudaGraph_t graph = nullptr;
       EVX_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -229,7 +245,7 @@ int evx_batch_launch(evx_batch *b) {
       cudaGraphDestroy(graph);
       if (e != cudaSuccess) { b->exec = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
       b->exec_nq = nq; b->exec_kmax = kmax; b->exec_tiles = tiles; b->exec_grid = grid;
-      b->exec_tile_roots = b->tile_roots; b->exec_graph = b->graph;
+      b->exec_tile_roots = b->tile_roots; b->exec_graph = b->graph; b->exec_limit = b->limit;
     }
     EVX_CUDA(cudaGraphLaunch(b->exec, b->stream));
   } else {
@@ -252,7 +268,8 @@ int evx_batch_result(evx_batch *b, uint64_t *counts, int n) {
   b->launched = false;
   const int nq = (int)b->queries.size();
   if (counts) {
-    for (int i = 0; i < n && i < nq; i++) counts[i] = b->counts_h[i];
+    for (int i = 0; i < n && i < nq; i++)
+      counts[i] = (b->limit && b->counts_h[b->max_q + i] > b->limit) ? UINT64_MAX : b->counts_h[i];
   }
   return EVX_OK;
 }

@@ -126,7 +126,7 @@ struct evx_worker {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int num_sms = 148;
-  // small device state: [0] u64 count, [2] int cursor, [3] int stop, [4..5] t range scratch
+  // small device state (u64 words): [0] count, [1] int cursor + int stop, [2] work meter
   unsigned long long *state_d = nullptr;
   unsigned long long *count_h = nullptr;  // pinned
   int *rows_d = nullptr;
@@ -140,6 +140,7 @@ struct evx_worker {
   SearchArgs args{};
   int64_t enum_cap = 0;
   uint64_t last_count = 0;
+  uint64_t limit = 0;  // work limit of later jobs (0 = none)
   // tuning
   int block = 256, blocks_per_sm = 0, roots_per_fetch = 32, steal_interval = 16, min_split = 2;
   int last_launches = 0;
@@ -345,7 +346,7 @@ int evx_worker_create(int device, void *stream, evx_worker **out) {
   }
   if (e == cudaSuccess) e = cudaMalloc(&w->state_d, 64);
   if (e == cudaSuccess) e = cudaMemset(w->state_d, 0, 64);
-  if (e == cudaSuccess) e = cudaMallocHost(&w->count_h, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMallocHost(&w->count_h, 2 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaEventCreate(&w->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&w->ev1);
   if (e != cudaSuccess) {
@@ -447,6 +448,8 @@ int evx_worker_take(evx_worker *w, const evx_graph *gh, int k, const int *mu, co
   a.count = w->state_d;
   a.cursor = reinterpret_cast<int *>(w->state_d + 1);
   a.stop = reinterpret_cast<int *>(w->state_d + 1) + 1;
+  a.limit = (unsigned long long)w->limit;
+  a.meter = w->state_d + 2;
   w->enum_cap = enum_cap;
   w->has_job = true;
   w->launched = false;
@@ -458,6 +461,7 @@ __global__ void reset_state_kernel(unsigned long long *count, int *cursor, int *
   *count = 0ull;
   *cursor = beg;  // the search's work queue: next unclaimed root tile
   *stop = 0;
+  count[2] = 0ull;  // work meter
 }
 }  // namespace evx
 
@@ -489,6 +493,9 @@ int evx_worker_launch(evx_worker *w) {
   EVX_CUDA(cudaEventRecord(w->ev1, w->stream));
   EVX_CUDA(cudaMemcpyAsync(w->count_h, a.count, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                            w->stream));
+  if (a.limit)
+    EVX_CUDA(cudaMemcpyAsync(w->count_h + 1, a.meter, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             w->stream));
   w->last_launches = launches;
   w->launched = true;
   return EVX_OK;
@@ -504,6 +511,14 @@ int evx_worker_result(evx_worker *w, uint64_t *count) {
   w->last_count = *w->count_h;
   *count = w->last_count;
   w->launched = false;
+  if (w->args.limit && w->count_h[1] > w->args.limit)
+    return fail(EVX_ERR_LIMIT, "work limit " + std::to_string(w->args.limit) + " exceeded");
+  return EVX_OK;
+}
+
+int evx_worker_set_limit(evx_worker *w, uint64_t max_work) {
+  if (!w) return fail(EVX_ERR_INVALID, "null worker");
+  w->limit = max_work;
   return EVX_OK;
 }
 

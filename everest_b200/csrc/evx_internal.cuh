@@ -102,6 +102,10 @@ struct LaunchArgs {
   int tile_roots;             // roots per tile (multiple of 32)
   int *cursor;                // next unclaimed tile
   unsigned long long *counts; // [nq] per-query counts
+  unsigned long long limit;   // work limit per query (0 = none): a query whose
+                              // meter passes it is stopped early
+  unsigned long long *meter;  // [nq] matches + queued partial matches per query
+                              // (maintained only when limit > 0)
 };
 
 // Search job arguments (one query).
@@ -120,6 +124,8 @@ struct SearchArgs {
   unsigned long long *count;  // [1] result / enumeration slot counter
   int *cursor;                // [1] next unclaimed root id
   int *stop;                  // [1] set when the enumeration cap is reached
+  unsigned long long limit;   // work limit (0 = none), count mode only
+  unsigned long long *meter;  // [1] matches + queued partial matches (limit > 0)
 };
 
 // Host-side graph object.

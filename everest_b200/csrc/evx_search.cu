@@ -69,15 +69,6 @@ __device__ __forceinline__ void put(int (&a)[N], int i, int v) {
 __device__ __forceinline__ int ld_eid(const int4 *p) { return __ldg(&p->x); }
 __device__ __forceinline__ int ld_t(const int4 *p) { return __ldg(&p->z); }
 
-// First position in [lo, hi) whose timestamp is greater than tv.
-__device__ __forceinline__ int first_t_after(const int4 *lst, int lo, int hi, int tv) {
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (ld_t(lst + mid) > tv) hi = mid; else lo = mid + 1;
-  }
-  return lo;
-}
-
 // (start, len) of the run of u->v edges in pair_rec; len 0 when absent.  The
 // probe sequence stops at the longest one the table build used.
 __device__ __forceinline__ int2 pair_find(const GraphView &g, int u, int v) {
@@ -188,6 +179,8 @@ struct alignas(16) WarpSmem {
   int4 task[(K > 2) ? (K - 2) : 1][kCap][2];
   int4 save[(K > 2) ? (K - 2) : 1][32][2];
   int nb[K];
+  int cur_q;               // index of the current query in the launch
+  int halt;                // set when the current query stops early (limit or cap)
 };
 
 // The previous matched edge of a task (what the next list opening needs).
@@ -205,6 +198,7 @@ struct Searcher {
   const GraphView &g;
   const MotifPlan &plan;   // the current query's plan (per-warp copy in shared memory)
   const EnumArgs &ea;
+  const LaunchArgs &la;
   WarpSmem<K> &sm;
   const int lane;
   const unsigned lt;
@@ -214,10 +208,43 @@ struct Searcher {
   // motif size (EXACT), else the table entry's
   __device__ __forceinline__ int kr() const { return EXACT ? K : kq; }
   unsigned long long cnt;
+  unsigned cand;  // adjacency records examined inside the window since the last meter update
 
-  __device__ Searcher(const GraphView &g_, const MotifPlan &p_, const EnumArgs &e_, WarpSmem<K> &s_,
-                      int lane_)
-      : g(g_), plan(p_), ea(e_), sm(s_), lane(lane_), lt((1u << lane_) - 1u), cnt(0) {}
+  __device__ Searcher(const GraphView &g_, const MotifPlan &p_, const EnumArgs &e_, const LaunchArgs &la_,
+                      WarpSmem<K> &s_, int lane_)
+      : g(g_), plan(p_), ea(e_), la(la_), sm(s_), lane(lane_), lt((1u << lane_) - 1u), cnt(0), cand(0) {}
+
+  // Add this warp's examined records to the current query's meter; returns
+  // the meter after the add.
+  __device__ __forceinline__ unsigned long long meter_add() {
+    unsigned long long c = cand;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+    unsigned long long tot = 0;
+    if (lane == 0) tot = atomicAdd(la.meter + sm.cur_q, c) + c;
+    cand = 0;
+    return __shfl_sync(kFull, tot, 0);
+  }
+
+  // Whether the current query has stopped: its enumeration cap was reached,
+  // or (with a work limit) its meter passed the limit.  The meter counts the
+  // adjacency records the search examines inside their time windows (not
+  // the one record past a window that ends each scan, nor binary-search
+  // probes): every such record is examined exactly once however the scans
+  // are split between lanes, so the meter's final value is fixed by the
+  // graph and the query.  Lanes add to it once one holds 512 records (so
+  // the records not yet added stay below 512 x the lanes of the grid); the
+  // total returned by that add is what is compared, so a query is stopped
+  // only once its final meter is known to exceed the limit.
+  __device__ __forceinline__ bool halted() {
+    if (sm.halt) return true;
+    if constexpr (ENUM) {
+      if (!ea.exact_total && *(volatile int *)ea.stop != 0) return true;
+    }
+    if (!la.limit) return false;
+    if (!__any_sync(kFull, cand >= 512u)) return false;
+    return meter_add() > la.limit;
+  }
 
   __device__ __forceinline__ void set_query(const QueryDesc &q) {
     strict = (q.flags & kQStrict) ? 1 : 0;
@@ -293,6 +320,13 @@ struct Searcher {
   template <int l>
   __device__ __forceinline__ void descend() {
     if constexpr (l + 1 < L) {
+      if (halted()) {
+        // drop the queued tasks; the caller ends its scan on sm.halt
+        __syncwarp();
+        if (lane == 0) { sm.halt = 1; sm.nb[l + 1] = 0; }
+        __syncwarp();
+        return;
+      }
       const int nb = sm.nb[l + 1];
       const int take = nb < 32 ? nb : 32;
       level<l + 1>(lane < take, lane, take);
@@ -342,6 +376,7 @@ struct Searcher {
         const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
         const int tlc = sm.root[root].z;
         cnt += (unsigned long long)pair_dir_window(g, ia, ib, strict ? p.t : p.eid, tlc, strict != 0);
+        ++cand;  // one directory lookup per task
       }
       return;
     }
@@ -421,14 +456,26 @@ struct Searcher {
               ++pos;
               if (rr[q].z > tl) {
                 pos = end;
-              } else if (structural_ok(rr[q].y, want, nmc, m)) {
-                ++cnt;
-                if (ENUM) { emit = true; last_eid = rr[q].x; }
+              } else {
+                ++cand;
+                if (structural_ok(rr[q].y, want, nmc, m)) {
+                  ++cnt;
+                  if (ENUM) { emit = true; last_eid = rr[q].x; }
+                }
               }
             }
           }
         }
-        if constexpr (ENUM) emit_row(emit, e, last_eid);
+        if constexpr (ENUM) {
+          if (emit_row(emit, e, last_eid)) {
+            // the cap is reached: end this scan and unwind the levels above
+            pos = end;
+            __syncwarp();
+            if (lane == 0) sm.halt = 1;
+            __syncwarp();
+            break;
+          }
+        }
       }
     } else if constexpr (l < L - 1) {
       // --------------------------------- scan, queue children, descend ----
@@ -452,6 +499,7 @@ struct Searcher {
             const int4 s0 = sm.save[l][lane][0], s1 = sm.save[l][lane][1];
             pos = s0.x; end = s0.y; want = s0.z; base = s0.w;
             slot = s1.x; root = s1.y; tl = s1.z; out = (s1.w & 1) != 0; steps = s1.w >> 1;
+            if (sm.halt) pos = end;  // the query stopped: unwind this level too
             Prev dummy;
             int rr;
             if (pos < end) reconstruct<l>(slot, m, e, dummy, rr);
@@ -467,8 +515,12 @@ struct Searcher {
           const int4 *lst = out ? g.out_rec : g.in_rec;
           rc = __ldg(lst + pos);
           ++pos;
-          if (rc.z > tl) pos = end;
-          else push = structural_ok(rc.y, want, nmc, m);
+          if (rc.z > tl) {
+            pos = end;
+          } else {
+            ++cand;
+            push = structural_ok(rc.y, want, nmc, m);
+          }
         }
         if (inline_here && same_pair) {
           if (push) {
@@ -551,9 +603,11 @@ struct Searcher {
     if (lane == donor) end = p0 + (int)((long long)w / parts);
   }
 
-  __device__ __forceinline__ void emit_row(bool emit, const int (&e)[KE], int last_eid) {
+  // Returns true (on every lane) once the enumeration cap is reached and the
+  // search stops there (no exact total requested).
+  __device__ __forceinline__ bool emit_row(bool emit, const int (&e)[KE], int last_eid) {
     const unsigned em = __ballot_sync(kFull, emit);
-    if (!em) return;
+    if (!em) return false;
     const int leader = __ffs(em) - 1;
     unsigned long long b0 = 0;
     if (lane == leader) b0 = atomicAdd(ea.count, (unsigned long long)__popc(em));
@@ -568,6 +622,7 @@ struct Searcher {
       }
       if (!ea.exact_total && s + 1 >= (unsigned long long)ea.cap) atomicExch(ea.stop, 1);
     }
+    return !ea.exact_total && b0 + (unsigned long long)__popc(em) >= (unsigned long long)ea.cap;
   }
 };
 
@@ -583,16 +638,20 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
   const int lane = threadIdx.x & 31;
   WarpSmem<K> &sm = smem[threadIdx.x >> 5];
   if (lane < K) sm.nb[lane] = 0;
+  if (lane == 0) { sm.halt = 0; sm.cur_q = 0; }
   __syncwarp();
-  Searcher<K, ENUM, EXACT> S(g, sm.q.plan, ea, sm, lane);
+  Searcher<K, ENUM, EXACT> S(g, sm.q.plan, ea, la, sm, lane);
   int cur_q = -1;
   auto flush = [&]() {
-    if (!ENUM && cur_q >= 0) {
-      unsigned long long c = S.cnt;
+    if (cur_q >= 0) {
+      if (!ENUM) {
+        unsigned long long c = S.cnt;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
-      if (lane == 0 && c) atomicAdd(la.counts + cur_q, c);
-      S.cnt = 0;
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(kFull, c, o);
+        if (lane == 0 && c) atomicAdd(la.counts + cur_q, c);
+        S.cnt = 0;
+      }
+      if (la.limit) S.meter_add();
     }
   };
   while (true) {
@@ -625,9 +684,16 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
       constexpr int W = sizeof(QueryDesc) / sizeof(int);
       int *dst = reinterpret_cast<int *>(&sm.q);
       for (int i = lane; i < W; i += 32) dst[i] = src[i];
+      if (lane == 0) sm.cur_q = q;
       __syncwarp();
       S.set_query(sm.q);
       cur_q = q;
+    }
+    if (la.limit) {
+      // a query past its limit: skip its remaining tiles
+      int over = 0;
+      if (lane == 0) over = *(volatile unsigned long long *)(la.meter + q) > la.limit;
+      if (__shfl_sync(kFull, over, 0)) continue;
     }
     const int rb = sm.q.root_beg + (t - sm.q.tile_beg) * la.tile_roots;
     const int re = min(rb + la.tile_roots, sm.q.root_end);
@@ -657,6 +723,14 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
         S.template level<0>(has, lane, 32);
       }
       __syncwarp();
+      if (sm.halt) {
+        // stopped inside this batch of roots: leave the tile (count mode);
+        // enumeration also stops claiming tiles through ea.stop
+        __syncwarp();
+        if (lane == 0) sm.halt = 0;
+        __syncwarp();
+        break;
+      }
       if (ENUM && *(volatile int *)ea.stop) break;
     }
   }
@@ -756,6 +830,8 @@ int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &a
   la.total_tiles = n > 0 ? (n + kSingleTileRoots - 1) / kSingleTileRoots : 0;
   la.cursor = args.cursor;
   la.counts = args.count;
+  la.limit = args.limit;
+  la.meter = args.meter;
   EnumArgs ea;
   ea.rows = args.rows;
   ea.cap = args.cap;

@@ -13,7 +13,12 @@ The reference answers one query at a time and re-uploads the graph for each
     admitted only when the device has room for their row buffers
     (cap x k x 4 bytes plus a reserve) and an enumeration slot is free;
 * completed work is detected without blocking (CUDA event queries), futures
-  are resolved and each request's latency (submit -> result) is recorded.
+  are resolved and each request's latency (submit -> result) is recorded;
+* an optional work limit bounds any one query (work = adjacency records
+  examined inside their time windows, fixed by the graph and the query): a
+  query past it is stopped on the device and resolved with
+  ``Result.limited`` set and no count (an enumeration keeps the rows it
+  wrote); every other result is exact.
 
 Results are independent of the mix: every query keeps its own counters in
 the batch (one per query) or its own worker.
@@ -40,21 +45,24 @@ class Request:
     delta: int
     enum_cap: int = 0
     flags: int = 0
+    beg: int = 0          # root edge ids [beg, end); end < 0 = to the last root
+    end: int = -1
     submitted: float = field(default_factory=time.perf_counter)
     future: Future = field(default_factory=Future)
 
 
 @dataclass
 class Result:
-    count: int
+    count: Optional[int]
     rows: Optional[np.ndarray] = None
     latency_s: float = 0.0
+    limited: bool = False  # stopped at the work limit (count is None)
 
 
 class Server:
     def __init__(self, device: int = 0, max_batch: int = 64, inflight_batches: int = 2,
                  enum_slots: int = 2, mem_reserve: int = 1 << 30, idle_sleep_s: float = 50e-6,
-                 backend=None):
+                 backend=None, limit: int = 0):
         # backend: the module providing Batch, Worker, DeviceGraph and
         # device_mem_info (the C-ABI binding; tests substitute a fake)
         self.be = backend if backend is not None else capi
@@ -68,12 +76,20 @@ class Server:
         self.enum_q: "collections.deque[Request]" = collections.deque()
         self.lock = threading.Lock()
         self.cv = threading.Condition(self.lock)
+        self.limit = int(limit)
         self.batches = [capi_.Batch(device, max_batch) for _ in range(inflight_batches)]
+        if self.limit:
+            for b in self.batches:
+                b.set_limit(self.limit)
         self.batch_reqs: List[Optional[List[Request]]] = [None] * inflight_batches
         self.enum_workers = [capi_.Worker(device) for _ in range(enum_slots)]
+        if self.limit:
+            for w in self.enum_workers:
+                w.set_limit(self.limit)
         self.enum_reqs: List[Optional[Request]] = [None] * enum_slots
         self.latencies: List[float] = []
         self.completed = 0
+        self.limited = 0
         self.batches_launched = 0
         self.first_submit: Optional[float] = None
         self.last_done: Optional[float] = None
@@ -86,10 +102,13 @@ class Server:
     def add_graph(self, name: str, host: capi.HostGraph) -> None:
         self.graphs[name] = self.be.DeviceGraph(host, self.device)
 
-    def submit(self, graph: str, mu, mv, delta: int, enum_cap: int = 0, flags: int = 0) -> Future:
+    def submit(self, graph: str, mu, mv, delta: int, enum_cap: int = 0, flags: int = 0, beg: int = 0,
+               end: int = -1) -> Future:
+        """Queue a query; roots are the edge ids [beg, end) (the whole graph
+        by default), as in the reference's MineJob(data, delta, beg, end)."""
         if graph not in self.graphs:
             raise KeyError(f"graph {graph!r} is not resident")
-        r = Request(graph, list(mu), list(mv), int(delta), int(enum_cap), int(flags))
+        r = Request(graph, list(mu), list(mv), int(delta), int(enum_cap), int(flags), int(beg), int(end))
         with self.cv:
             if self.first_submit is None:
                 self.first_submit = r.submitted
@@ -100,7 +119,7 @@ class Server:
     def stats(self) -> dict:
         lat = np.array(self.latencies) if self.latencies else np.zeros(1)
         span = (self.last_done - self.first_submit) if (self.last_done and self.first_submit) else 0.0
-        return {"completed": self.completed, "batches": self.batches_launched,
+        return {"completed": self.completed, "limited": self.limited, "batches": self.batches_launched,
                 "queries_per_s": self.completed / span if span > 0 else 0.0,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "p999_ms": float(np.percentile(lat, 99.9) * 1e3), "max_ms": float(lat.max() * 1e3)}
@@ -138,6 +157,7 @@ class Server:
         res.latency_s = now - r.submitted
         self.latencies.append(res.latency_s)
         self.completed += 1
+        self.limited += 1 if res.limited else 0
         self.last_done = now
         r.future.set_result(res)
 
@@ -150,37 +170,44 @@ class Server:
                 b.clear()
                 self.batch_reqs[i] = None
                 for r, c in zip(reqs, counts):
-                    self._finish(r, Result(c))
+                    lim = c == capi.LIMITED
+                    self._finish(r, Result(None if lim else c, limited=lim))
                 progressed = True
         for i, w in enumerate(self.enum_workers):
             r = self.enum_reqs[i]
             if r is not None and w.done():
-                c = w.result()
+                try:
+                    c, lim = w.result(), False
+                except capi.LimitExceeded:
+                    c, lim = None, True
                 rows = w.enum_rows(r.enum_cap)
                 self.enum_reqs[i] = None
-                self._finish(r, Result(c, rows))
+                self._finish(r, Result(c, rows, limited=lim))
                 progressed = True
         return progressed
 
     def _admit(self) -> bool:
         progressed = False
-        # count queries: fill free batch slots (one graph per batch)
+        # count queries: fill free batch slots.  A batch holds one graph and
+        # one motif size: the persistent kernel is instantiated for the
+        # largest motif of its batch, and a smaller motif run in a larger
+        # instantiation pays for its registers and shared memory.
         for i, b in enumerate(self.batches):
             if self.batch_reqs[i] is not None:
                 continue
             with self.lock:
                 if not self.count_q:
                     break
-                g = self.count_q[0].graph
+                key = (self.count_q[0].graph, len(self.count_q[0].mu))
                 take = []
                 rest = collections.deque()
                 while self.count_q and len(take) < self.max_batch:
                     r = self.count_q.popleft()
-                    (take if r.graph == g else rest).append(r)
+                    (take if (r.graph, len(r.mu)) == key else rest).append(r)
                 rest.extend(self.count_q)
                 self.count_q = rest
             for r in take:
-                b.add(self.graphs[r.graph], r.mu, r.mv, r.delta, 0, -1, r.flags)
+                b.add(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.flags)
             b.launch()
             self.batch_reqs[i] = take
             self.batches_launched += 1
@@ -199,7 +226,7 @@ class Server:
                 break  # wait for running work to release memory
             with self.lock:
                 self.enum_q.popleft()
-            w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, 0, -1, r.enum_cap, r.flags)
+            w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags)
             w.launch()
             self.enum_reqs[i] = r
             progressed = True

@@ -5,7 +5,9 @@ Each workload is a graph from ``synth.SPECS`` plus a list of queries
 (relabeled motif edges, delta, count or enumerate cap)."""
 from __future__ import annotations
 
-from typing import Dict, List
+from typing import Dict, List, Sequence, Tuple
+
+import numpy as np
 
 from . import synth
 
@@ -29,3 +31,55 @@ def queries(name: str) -> List[dict]:
                         "delta": wl["delta"]})
         return out
     raise KeyError(name)
+
+
+# ------------------------------------------------- batch and serving mixes --
+
+def mixed_queries(n: int, seed: int, edge_range: Tuple[int, int], node_range: Tuple[int, int],
+                  graphs: Sequence[Tuple[str, int]], window: int, deltas: Sequence[int] = (),
+                  delta_range: Tuple[int, int] = (0, 0), enum_frac: float = 0.0,
+                  cap_range: Tuple[float, float] = (1e4, 1e6)) -> List[dict]:
+    """``n`` seeded queries over resident graphs.
+
+    Each query: a random connected pattern (``synth.random_patterns``, edges
+    and nodes drawn from the inclusive ranges), a graph (round robin over
+    ``graphs`` = [(name, num_edges)]), a root window of ``window`` consecutive
+    edge ids at a uniform random start (the reference's MineJob(data, delta,
+    beg, end) root range; a window of edges is a window of time, the edge
+    list being sorted by timestamp), delta from ``deltas`` round robin or
+    log-uniform in ``delta_range``, and with probability ``enum_frac`` an
+    enumeration with a cap log-uniform in ``cap_range`` (0 = count)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pats = synth.random_patterns(n, edge_range, node_range, seed=seed) if n <= 200 else \
+        synth.random_patterns(200, edge_range, node_range, seed=seed)
+    out = []
+    for i in range(n):
+        p = pats[int(rng.integers(0, len(pats)))] if n > len(pats) else pats[i]
+        gname, E = graphs[i % len(graphs)]
+        beg = int(rng.integers(0, max(1, E - window)))
+        if deltas:
+            d = int(deltas[i % len(deltas)])
+        else:
+            d = int(np.exp(rng.uniform(np.log(delta_range[0]), np.log(delta_range[1]))))
+        cap = 0
+        if enum_frac and rng.random() < enum_frac:
+            cap = int(np.exp(rng.uniform(np.log(cap_range[0]), np.log(cap_range[1]))))
+        out.append({"graph": gname, "mu": [a for a, b in p], "mv": [b for a, b in p], "delta": d,
+                    "beg": beg, "end": min(E, beg + window), "cap": cap})
+    return out
+
+
+def batch_queries(window: int = 1_000_000, n: int = 64) -> List[dict]:
+    """64 queries mixing 3- and 4-edge patterns on 2-4 nodes, delta cycling
+    through {3600, 86400, 604800}, on the 2.6M-node / 36M-edge graph."""
+    spec = synth.SPECS["bursty-2.6m-36m"]
+    return mixed_queries(n, 3, (3, 4), (2, 4), [(spec.name, spec.num_edges)], window,
+                         deltas=(3600, 86400, 604800))
+
+
+def serve_queries(window: int = 100_000, n: int = 10_000) -> List[dict]:
+    """Serving stream: 3-5-edge patterns on 2-4 nodes over the 7.8M- and
+    63M-edge graphs, delta log-uniform in [600, 604800], 20% enumerations
+    with a cap log-uniform in [1e4, 1e6]."""
+    graphs = [(synth.SPECS[k].name, synth.SPECS[k].num_edges) for k in ("bursty-1.1m-7.8m", "bursty-6m-63m")]
+    return mixed_queries(n, 5, (3, 5), (2, 4), graphs, window, delta_range=(600, 604800), enum_frac=0.2)

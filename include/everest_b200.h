@@ -34,6 +34,7 @@ extern "C" {
 #define EVX_ERR_STATE (-6)     /* call out of order (e.g. run before take) */
 #define EVX_ERR_TIMEOUT (-7)   /* a bounded device wait gave up */
 #define EVX_ERR_NODEVICE (-8)  /* no CUDA device */
+#define EVX_ERR_LIMIT (-9)     /* a query passed its work limit (evx_*_set_limit) */
 
 /* Largest motif the kernels are instantiated for. */
 #define EVX_MAX_MOTIF_EDGES 8
@@ -169,6 +170,21 @@ EVX_API int evx_worker_set_tuning(evx_worker *w, int block, int blocks_per_sm,
  * and device milliseconds measured with CUDA events around them. */
 EVX_API int evx_worker_last_stats(evx_worker *w, int *kernel_launches, float *device_ms);
 
+/* Work limit for later jobs of this worker (0 = none, the default).  No
+ * counterpart in the reference, whose searches always run to the end.  A
+ * serving caller uses it to bound the work of any one query.  The work
+ * measure ("meter") is the number of adjacency records the search examines
+ * inside their time windows; every such record is examined exactly once
+ * however the scans are split between lanes, so the meter is fixed by the
+ * graph and the query, not by scheduling.  Once the meter is known to
+ * exceed max_work the search stops, and evx_worker_run / evx_worker_result
+ * return EVX_ERR_LIMIT with *count set to the matches counted so far (a
+ * lower bound; an enumeration keeps the rows written so far, readable with
+ * evx_worker_enum_rows).  A query whose meter stays <= max_work is never
+ * stopped and its result is exact, so whether a query is stopped does not
+ * depend on scheduling. */
+EVX_API int evx_worker_set_limit(evx_worker *w, uint64_t max_work);
+
 /* -------------------------------------------------------------- batches --
  * Many count queries against one resident graph in a single persistent
  * launch (no counterpart in the reference, whose batch driver re-generates,
@@ -195,6 +211,12 @@ EVX_API int evx_batch_query(evx_batch *b, int *done);
 EVX_API int evx_batch_set_tuning(evx_batch *b, int tile_roots, int blocks_per_sm, int steal_interval,
                                  int min_split, int use_graph, int reserved);
 EVX_API int evx_batch_last_stats(evx_batch *b, int *kernel_launches, float *device_ms);
+
+/* Work limit per query of this batch (0 = none): evx_worker_set_limit's
+ * rule, query by query.  evx_batch_result still returns EVX_OK; it writes
+ * UINT64_MAX as the count of each stopped query and the exact count of
+ * every other query. */
+EVX_API int evx_batch_set_limit(evx_batch *b, uint64_t max_work);
 
 /* ------------------------------------------------- allocation-free count --
  * No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -7,7 +7,7 @@ import time
 import numpy as np
 import pytest
 
-from everest_b200 import serve, synth
+from everest_b200 import capi, serve, synth
 from oracle import oracle as O
 
 
@@ -35,12 +35,22 @@ class FakeBackend:
             def __init__(self):
                 self.q = []
                 self.t_done = None
+                self.limit = 0
+
+            def set_limit(self, n):
+                self.limit = n
 
             def add(self, g, mu, mv, d, beg, end, flags):
-                self.q.append((g, mu, mv, d))
+                self.q.append((g, mu, mv, d, beg, end))
 
             def launch(self):
-                self.res = [O.count(be.graphs[g], mu, mv, d)[0] for g, mu, mv, d in self.q]
+                self.res = []
+                for g, mu, mv, d, beg, end in self.q:
+                    gr = be.graphs[g]
+                    hi = O.default_roots(gr, len(mu))[1] if end < 0 else min(end, O.default_roots(gr, len(mu))[1])
+                    c = O.count(gr, mu, mv, d, roots=(beg, max(beg, hi)))[0]
+                    # the fake's work measure is the count itself
+                    self.res.append(capi.LIMITED if self.limit and c > self.limit else c)
                 self.t_done = time.perf_counter() + 0.002
 
             def done(self):
@@ -60,6 +70,9 @@ class FakeBackend:
         be = self
 
         class W:
+            def set_limit(self, n):
+                self.limit = n
+
             def take(self, g, mu, mv, d, beg, end, cap, flags):
                 self.args = (g, mu, mv, d, cap)
 
@@ -134,4 +147,30 @@ def test_unknown_graph_rejected(graph):
     srv = serve.Server(backend=be)
     with pytest.raises(KeyError):
         srv.submit("nope", [0, 1], [1, 0], 5)
+    srv.close()
+
+
+def test_root_ranges_and_count_limit(graph):
+    # windows of roots, and a limit that stops the largest queries: those
+    # come back flagged, every other count is exact
+    be = FakeBackend({"g": graph}, free_bytes=1 << 40)
+    E = graph.u.size
+    qs = [([0, 1, 2], [1, 2, 0], 3000, 0, E // 2), ([0, 0, 0], [1, 2, 1], 3000, E // 3, E),
+          ([0, 1], [1, 0], 4000, 100, 900), ([0, 0], [1, 1], 30_000, 0, -1)]
+    exact = []
+    for mu, mv, d, beg, end in qs:
+        hi = O.default_roots(graph, len(mu))[1] if end < 0 else min(end, O.default_roots(graph, len(mu))[1])
+        exact.append(O.count(graph, mu, mv, d, roots=(beg, hi))[0])
+    limit = sorted(exact)[-2]  # the largest query passes it, the others do not
+    srv = serve.Server(max_batch=4, inflight_batches=1, enum_slots=1, mem_reserve=0, backend=be, limit=limit)
+    srv.add_graph("g", "g")
+    futs = [srv.submit("g", mu, mv, d, beg=beg, end=end) for mu, mv, d, beg, end in qs]
+    srv.drain(60)
+    for f, c in zip(futs, exact):
+        r = f.result(1)
+        if c > limit:
+            assert r.limited and r.count is None
+        else:
+            assert not r.limited and r.count == c
+    assert srv.stats()["limited"] == sum(c > limit for c in exact) == 1
     srv.close()
