@@ -358,6 +358,9 @@ def run_gpu_arm(args):
                 "ms_per_step": e_total / args.steps},
         "gpu_launches": launches,
         "per_query_ms": per_query_ms,
+        "per_query_tuning": {k: "bps%d/steal%d/split%d/flags%d" % (c["blocks_per_sm"], c["steal_interval"],
+                                                                     c["min_split"], c["flags"])
+                             for k, c in tuned.items()},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs",

@@ -11,8 +11,8 @@ sample, which is checked) and caches the winner per key:
 
 Knobs: resident blocks per SM (0 = occupancy), intra-warp rebalance interval
 and minimum split width ("steal granularity"), and how the last edge is
-counted: range arithmetic on the pair index, a pair-directory lookup per
-partial match, or a scan ("tail-expansion depth").  Batches are tuned on
+counted: range arithmetic on the pair index, a pair hash-table or
+pair-directory lookup per partial match, or a scan ("tail-expansion depth").  Batches are tuned on
 their tile size.
 """
 from __future__ import annotations
@@ -34,6 +34,8 @@ CANDIDATES = [
     {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_NO_PAIR_INDEX},
     {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_PAIR_DIR},
     {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_PAIR_DIR},
+    {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_CLOSING_SCAN},
+    {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_CLOSING_SCAN},
     {"blocks_per_sm": 4, "steal_interval": 16, "min_split": 2, "flags": 0},
 ]
 BATCH_TILES = (64, 128, 256, 512)

@@ -28,6 +28,7 @@ FLAG_EXACT_TOTAL = 2
 FLAG_NO_STEAL = 4
 FLAG_NO_PAIR_INDEX = 8
 FLAG_PAIR_DIR = 16
+FLAG_CLOSING_SCAN = 32
 MAX_MOTIF_EDGES = 8
 
 # every symbol include/everest_b200.h declares

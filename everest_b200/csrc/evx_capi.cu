@@ -99,8 +99,10 @@ int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
 // mode) for a closing last edge: when it closes on two nodes mapped before
 // the second-to-last edge (its pair is fixed per partial match:
 // kQInlineLast), when it repeats the second-to-last edge's endpoints (its
-// pair run is the one the matched edge sits in: kQSamePair), and, on
-// request, through the per-node pair directory (kQPairDir).
+// pair run is the one the matched edge sits in: kQSamePair), and for a
+// closing edge whose pair changes with every partial match: one lookup per
+// partial match in the pair hash table (kQPairHash, the default) or, on
+// request, in the per-node pair directory (kQPairDir).
 int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
   const int k = plan.k;
   if (enumerate || (flags & EVX_FLAG_NO_PAIR_INDEX) || k < 2) return 0;
@@ -113,6 +115,7 @@ int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
     if (plan_a(wp) == plan_a(wl) && plan_b(wp) == plan_b(wl)) return kQSamePair;
     // the pair depends on the node the second-to-last edge maps
     if (flags & EVX_FLAG_PAIR_DIR) return kQPairDir;
+    if (!(flags & EVX_FLAG_CLOSING_SCAN)) return kQPairHash;
   }
   return 0;
 }

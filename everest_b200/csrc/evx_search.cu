@@ -203,10 +203,14 @@ struct Searcher {
   const int lane;
   const unsigned lt;
   // the current query's options (reloaded when the warp switches queries)
-  int strict = 0, inline_last = 0, same_pair = 0, pair_dir = 0, steal_interval = 0, min_split = 2, kq = K;
+  // the current query's options: kQ* flags and rebalance interval in
+  // registers, the rest read from its shared-memory copy
+  int qf = 0;
+  int si = 0;
   // motif edges of the current query: K itself when the launch has one
   // motif size (EXACT), else the table entry's
-  __device__ __forceinline__ int kr() const { return EXACT ? K : kq; }
+  __device__ __forceinline__ int kr() const { return EXACT ? K : sm.q.plan.k; }
+  __device__ __forceinline__ bool strict_() const { return (qf & kQStrict) != 0; }
   unsigned long long cnt;
   unsigned cand;  // adjacency records examined inside the window since the last meter update
 
@@ -247,13 +251,8 @@ struct Searcher {
   }
 
   __device__ __forceinline__ void set_query(const QueryDesc &q) {
-    strict = (q.flags & kQStrict) ? 1 : 0;
-    inline_last = (q.flags & kQInlineLast) ? 1 : 0;
-    same_pair = (q.flags & kQSamePair) ? 1 : 0;
-    pair_dir = (q.flags & kQPairDir) ? 1 : 0;
-    steal_interval = q.steal_interval;
-    min_split = q.min_split;
-    kq = q.plan.k;
+    qf = q.flags;
+    si = q.steal_interval;
   }
 
   // Node images and edge ids of the partial match in slot s of level l.
@@ -367,15 +366,30 @@ struct Searcher {
     }
     int tl = sm.root[root].z;
 
+    // ---------------------------- last level through the pair hash table ----
+    if (!ENUM && (qf & kQPairHash) && l == kr() - 2) {
+      // the closing last edge of each lane's task: one hash probe sequence
+      // for its pair's run, then the run's entries after the previous edge
+      // and inside the window (runs are short; 32 lanes probe in parallel)
+      if (has) {
+        const int w = plan.info[l];
+        const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
+        const int2 f = pair_find(g, ia, ib);
+        cnt += (unsigned long long)pair_window(g, f.x, f.y, strict_() ? p.t : p.eid, tl, strict_());
+        ++cand;  // one lookup per task
+      }
+      return;
+    }
+
     // --------------------------- last level through the pair directory ----
-    if (!ENUM && pair_dir && l == kr() - 2) {
+    if (!ENUM && (qf & kQPairDir) && l == kr() - 2) {
       // the closing last edge of each lane's task: count its static pair's
       // run inside the window (converged across the batch's 32 tasks)
       if (has) {
         const int w = plan.info[l];
         const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
         const int tlc = sm.root[root].z;
-        cnt += (unsigned long long)pair_dir_window(g, ia, ib, strict ? p.t : p.eid, tlc, strict != 0);
+        cnt += (unsigned long long)pair_dir_window(g, ia, ib, strict_() ? p.t : p.eid, tlc, strict_());
         ++cand;  // one directory lookup per task
       }
       return;
@@ -412,7 +426,7 @@ struct Searcher {
         sc = (p.dst == ib) ? p.pip + 1 : -1;
       }
       end = hi;
-      if (!strict && sc >= 0) {
+      if (!strict_() && sc >= 0) {
         pos = sc;
       } else if (lo < hi) {
         blo = lo; bhi = hi; searching = true;
@@ -422,12 +436,12 @@ struct Searcher {
     }
     // first record after the previous edge (by id; by time in strict mode)
     {
-      const int key = strict ? p.t : p.eid;
+      const int key = strict_() ? p.t : p.eid;
       while (__any_sync(kFull, searching)) {
         if (searching) {
           const int4 *lst = out ? g.out_rec : g.in_rec;
           const int mid = (blo + bhi) >> 1;
-          const int v = strict ? ld_t(lst + mid) : ld_eid(lst + mid);
+          const int v = strict_() ? ld_t(lst + mid) : ld_eid(lst + mid);
           if (v > key) bhi = mid; else blo = mid + 1;
           if (blo >= bhi) { searching = false; pos = blo; }
         }
@@ -440,7 +454,7 @@ struct Searcher {
       while (true) {
         const unsigned act = __ballot_sync(kFull, pos < end);
         if (!act) break;
-        if (act != kFull && steal_interval && ((++steps) & (steal_interval - 1)) == 0)
+        if (act != kFull && si && ((++steps) & (si - 1)) == 0)
           rebalance(act, pos, end, want, out, base, slot, root, tl, m, e);
         bool emit = false;
         int last_eid = 0;
@@ -481,7 +495,7 @@ struct Searcher {
       // --------------------------------- scan, queue children, descend ----
       // The level before the last one counts a closing last edge inline by
       // range arithmetic on the pair index (count mode only).
-      const bool inline_here = (l == kr() - 3) && !ENUM && (inline_last || same_pair);
+      const bool inline_here = (l == kr() - 3) && !ENUM && (qf & (kQInlineLast | kQSamePair));
       const int wl = plan.info[kr() - 2];
       const int la = plan_a(wl), lb = plan_b(wl);
       int ca = -1, cb = -1, ctl = 0, cs = 0, cub = 0, ckey = 0;  // this lane's pair cursor
@@ -507,7 +521,7 @@ struct Searcher {
           }
         }
         if (!act) break;
-        if (act != kFull && steal_interval && ((++steps) & (steal_interval - 1)) == 0)
+        if (act != kFull && si && ((++steps) & (si - 1)) == 0)
           rebalance(act, pos, end, want, out, base, slot, root, tl, m, e);
         bool push = false;
         int4 rc = make_int4(0, 0, 0, 0);
@@ -522,13 +536,13 @@ struct Searcher {
             push = structural_ok(rc.y, want, nmc, m);
           }
         }
-        if (inline_here && same_pair) {
+        if (inline_here && (qf & kQSamePair)) {
           if (push) {
             // the last edge repeats this edge's endpoints: count the rest of
             // the matched edge's own pair run inside the window
             const int2 pl = __ldg(g.pair_loc + rc.x);
             int lo = pl.x + 1;
-            if (strict) lo = pair_first_t_after(g, lo, pl.y, rc.z);
+            if (strict_()) lo = pair_first_t_after(g, lo, pl.y, rc.z);
             cnt += (unsigned long long)(pair_gallop_t_after(g, lo, pl.y, tl) - lo);
           }
         } else if (inline_here) {
@@ -537,18 +551,18 @@ struct Searcher {
             // pair run is fixed for the task: keep a cursor into it that only
             // moves forward as this lane's candidates advance
             const int ia = sel(m, la), ib = sel(m, lb);
-            const int key = strict ? rc.z : rc.x;
+            const int key = strict_() ? rc.z : rc.x;
             if (ia != ca || ib != cb || tl != ctl || key < ckey) {
               const int2 f = pair_find(g, ia, ib);
               ca = ia; cb = ib; ctl = tl;
               cub = pair_first_t_after(g, f.x, f.x + f.y, tl);
-              cs = pair_first_key_after(g, f.x, cub, key, strict != 0);
+              cs = pair_first_key_after(g, f.x, cub, key, strict_());
             } else {
               // a few steps forward; fall back to a search for long jumps
               int steps_left = 4;
               while (cs < cub && steps_left-- > 0 &&
-                     (strict ? __ldg(&g.pair_rec[cs].y) : __ldg(&g.pair_rec[cs].x)) <= key) ++cs;
-              if (steps_left < 0) cs = pair_first_key_after(g, cs, cub, key, strict != 0);
+                     (strict_() ? __ldg(&g.pair_rec[cs].y) : __ldg(&g.pair_rec[cs].x)) <= key) ++cs;
+              if (steps_left < 0) cs = pair_first_key_after(g, cs, cub, key, strict_());
             }
             ckey = key;
             cnt += (unsigned long long)(cub - cs);
@@ -567,7 +581,7 @@ struct Searcher {
                                             int (&e)[EE]) {
     const int width = end - pos;
     const unsigned wmax = __reduce_max_sync(kFull, (unsigned)(width > 0 ? width : 0));
-    if ((int)wmax < min_split) return;
+    if ((int)wmax < sm.q.min_split) return;
     const int donor = __ffs(__ballot_sync(kFull, (unsigned)width == wmax)) - 1;
     const unsigned idle = ~act;
     const int nthief = min(__popc(idle), (int)wmax - 1);
@@ -709,15 +723,15 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
         }
       }
       __syncwarp();
-      if (!ENUM && S.kr() == 2 && S.inline_last) {
+      if (!ENUM && S.kr() == 2 && (S.qf & kQInlineLast)) {
         // the only searched edge closes on the root's endpoints
         if (has) {
           const int4 rt = sm.root[lane];
           const int w = sm.q.plan.info[0];
           const int ia = plan_a(w) == 0 ? rt.x : rt.y, ib = plan_b(w) == 0 ? rt.x : rt.y;
           const int2 f = pair_find(g, ia, ib);
-          const int key = S.strict ? rt.z - delta : rt.w;
-          S.cnt += (unsigned long long)pair_window(g, f.x, f.y, key, rt.z, S.strict != 0);
+          const int key = S.strict_() ? rt.z - delta : rt.w;
+          S.cnt += (unsigned long long)pair_window(g, f.x, f.y, key, rt.z, S.strict_());
         }
       } else {
         S.template level<0>(has, lane, 32);

@@ -45,8 +45,11 @@ extern "C" {
 #define EVX_FLAG_EXACT_TOTAL 2u  /* enumerate: keep counting past the cap */
 #define EVX_FLAG_NO_STEAL 4u     /* disable intra-warp work stealing */
 #define EVX_FLAG_NO_PAIR_INDEX 8u /* count the last edge by scanning, not range arithmetic */
-#define EVX_FLAG_PAIR_DIR 16u     /* closing last edge whose pair changes per candidate: look the
-                                     pair up in the per-node directory instead of scanning */
+/* A closing last edge whose pair changes with every partial match is counted
+ * by one pair hash-table lookup per partial match by default; these select
+ * the per-node pair directory, or a scan of the shorter endpoint list. */
+#define EVX_FLAG_PAIR_DIR 16u
+#define EVX_FLAG_CLOSING_SCAN 32u
 
 typedef struct evx_graph evx_graph;   /* a graph resident on one device */
 typedef struct evx_worker evx_worker; /* per-device search worker */

@@ -62,6 +62,10 @@ def test_golden_small_graph_counts(golden, small_graphs, worker):
                 got3 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
                                  flags=capi.FLAG_PAIR_DIR)
                 assert got3 == c["count"], (gname, c["motif"], c["delta"], got3, "pair dir")
+            if n % 3 == 0:  # the scanned closing edge on a subset
+                got4 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
+                                 flags=capi.FLAG_CLOSING_SCAN)
+                assert got4 == c["count"], (gname, c["motif"], c["delta"], got4, "closing scan")
             if n % 7 == 0:  # the scanning last level on a subset
                 got2 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
                                  flags=capi.FLAG_NO_PAIR_INDEX)
@@ -95,6 +99,12 @@ def test_golden_zipf_200k(golden, worker):
         assert gpu_count(worker, dg, p["mu"], p["mv"], p["delta"],
                          flags=capi.FLAG_PAIR_DIR) == p["count"], p["motif"]
         assert gpu_count(worker, dg, p["mu"], p["mv"], p["delta"],
+                         flags=capi.FLAG_CLOSING_SCAN) == p["count"], p["motif"]
+        assert gpu_count(worker, dg, p["mu"], p["mv"], p["delta"],
+                         flags=capi.FLAG_STRICT_TS | capi.FLAG_CLOSING_SCAN) == gpu_count(
+            worker, dg, p["mu"], p["mv"], p["delta"],
+            flags=capi.FLAG_STRICT_TS | capi.FLAG_NO_PAIR_INDEX), p["motif"]
+        assert gpu_count(worker, dg, p["mu"], p["mv"], p["delta"],
                          flags=capi.FLAG_STRICT_TS) == gpu_count(
             worker, dg, p["mu"], p["mv"], p["delta"],
             flags=capi.FLAG_STRICT_TS | capi.FLAG_NO_PAIR_INDEX), p["motif"]
@@ -116,10 +126,11 @@ def test_random_tiny_vs_brute_force(worker):
         delta = int(rng.integers(0, 10))
         want = len(O.brute_force(u, v, t, mu, mv, delta))
         dg = device_graph(u, v, t)
-        for flags in (0, capi.FLAG_NO_STEAL, capi.FLAG_NO_PAIR_INDEX, capi.FLAG_PAIR_DIR):
+        for flags in (0, capi.FLAG_NO_STEAL, capi.FLAG_NO_PAIR_INDEX, capi.FLAG_PAIR_DIR, capi.FLAG_CLOSING_SCAN):
             assert gpu_count(worker, dg, mu, mv, delta, flags=flags) == want, (trial, pat, delta, flags)
         strict = len(O.brute_force(u, v, t, mu, mv, delta, strict_ts=True))
         assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS) == strict
+        assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS | capi.FLAG_CLOSING_SCAN) == strict
         dg.free()
 
 
