@@ -44,6 +44,12 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kCap = 64;        // task slots per buffered level per warp
 constexpr int kBlock = 128;     // threads per block
 constexpr int kWarps = kBlock / 32;
+// Records each lane loads per round in a non-last level's scan.
+#ifndef EVX_SCAN_WIDE
+#define EVX_SCAN_WIDE 2
+#endif
+constexpr int kScanWide = EVX_SCAN_WIDE;
+
 // resident blocks per SM the register budget aims for (deeper motifs keep
 // more per-level state live)
 #ifndef EVX_MINB3
@@ -499,6 +505,19 @@ struct Searcher {
       const int wl = plan.info[kr() - 2];
       const int la = plan_a(wl), lb = plan_b(wl);
       int ca = -1, cb = -1, ctl = 0, cs = 0, cub = 0, ckey = 0;  // this lane's pair cursor
+      if (inline_here && (qf & kQInlineLast) && has && pos < end) {
+        // the closing pair is fixed for the task: place the cursor on its
+        // run's entries after the previous edge inside the window once; when
+        // there are none, no candidate of the task can close and its scan is
+        // skipped
+        const int ia = sel(m, la), ib = sel(m, lb);
+        const int key = strict_() ? p.t : p.eid;
+        const int2 f = pair_find(g, ia, ib);
+        ca = ia; cb = ib; ctl = tl; ckey = key;
+        cub = pair_first_t_after(g, f.x, f.x + f.y, tl);
+        cs = pair_first_key_after(g, f.x, cub, key, strict_());
+        if (cs >= cub) pos = end;
+      }
       while (true) {
         const unsigned act = __ballot_sync(kFull, pos < end);
         if (!inline_here) {
@@ -523,52 +542,94 @@ struct Searcher {
         if (!act) break;
         if (act != kFull && si && ((++steps) & (si - 1)) == 0)
           rebalance(act, pos, end, want, out, base, slot, root, tl, m, e);
-        bool push = false;
-        int4 rc = make_int4(0, 0, 0, 0);
-        if (pos < end) {
+        // the next kScanWide records of every lane's range in one round of
+        // loads (one memory latency instead of kScanWide), then processed
+        // one at a time; records not processed before a descend are
+        // loaded again after it
+        int4 rw[kScanWide];
+        {
           const int4 *lst = out ? g.out_rec : g.in_rec;
-          rc = __ldg(lst + pos);
-          ++pos;
-          if (rc.z > tl) {
-            pos = end;
-          } else {
-            ++cand;
-            push = structural_ok(rc.y, want, nmc, m);
+#pragma unroll
+          for (int q = 0; q < kScanWide; q++) {
+            rw[q] = make_int4(0, 0, 0, 0);
+            if (pos + q < end) rw[q] = __ldg(lst + pos + q);
           }
         }
-        if (inline_here && (qf & kQSamePair)) {
-          if (push) {
-            // the last edge repeats this edge's endpoints: count the rest of
-            // the matched edge's own pair run inside the window
-            const int2 pl = __ldg(g.pair_loc + rc.x);
-            int lo = pl.x + 1;
-            if (strict_()) lo = pair_first_t_after(g, lo, pl.y, rc.z);
-            cnt += (unsigned long long)(pair_gallop_t_after(g, lo, pl.y, tl) - lo);
-          }
-        } else if (inline_here) {
-          if (push) {
-            // the last edge joins two nodes mapped before this level, so its
-            // pair run is fixed for the task: keep a cursor into it that only
-            // moves forward as this lane's candidates advance
-            const int ia = sel(m, la), ib = sel(m, lb);
-            const int key = strict_() ? rc.z : rc.x;
-            if (ia != ca || ib != cb || tl != ctl || key < ckey) {
-              const int2 f = pair_find(g, ia, ib);
-              ca = ia; cb = ib; ctl = tl;
-              cub = pair_first_t_after(g, f.x, f.x + f.y, tl);
-              cs = pair_first_key_after(g, f.x, cub, key, strict_());
-            } else {
-              // a few steps forward; fall back to a search for long jumps
-              int steps_left = 4;
-              while (cs < cub && steps_left-- > 0 &&
-                     (strict_() ? __ldg(&g.pair_rec[cs].y) : __ldg(&g.pair_rec[cs].x)) <= key) ++cs;
-              if (steps_left < 0) cs = pair_first_key_after(g, cs, cub, key, strict_());
+        if (inline_here) {
+          // count only, nothing queued: take every loaded record's verdict
+          // first, then issue the closing-edge lookups of all of them
+          bool ok[kScanWide];
+#pragma unroll
+          for (int q = 0; q < kScanWide; q++) {
+            ok[q] = false;
+            if (pos < end) {
+              ++pos;
+              if (rw[q].z > tl) {
+                pos = end;
+              } else {
+                ++cand;
+                ok[q] = structural_ok(rw[q].y, want, nmc, m);
+              }
             }
-            ckey = key;
-            cnt += (unsigned long long)(cub - cs);
+          }
+          if (qf & kQSamePair) {
+            // the last edge repeats the matched edge's endpoints: count the
+            // rest of that edge's own pair run inside the window
+            int2 pl[kScanWide];
+#pragma unroll
+            for (int q = 0; q < kScanWide; q++)
+              pl[q] = ok[q] ? __ldg(g.pair_loc + rw[q].x) : make_int2(0, 0);
+#pragma unroll
+            for (int q = 0; q < kScanWide; q++) {
+              if (ok[q]) {
+                int lo = pl[q].x + 1;
+                if (strict_()) lo = pair_first_t_after(g, lo, pl[q].y, rw[q].z);
+                cnt += (unsigned long long)(pair_gallop_t_after(g, lo, pl[q].y, tl) - lo);
+              }
+            }
+          } else {
+            // the last edge joins two nodes mapped before this level, so its
+            // pair run is fixed for the task: a cursor into it only moves
+            // forward as this lane's candidates advance
+#pragma unroll
+            for (int q = 0; q < kScanWide; q++) {
+              if (ok[q]) {
+                const int ia = sel(m, la), ib = sel(m, lb);
+                const int key = strict_() ? rw[q].z : rw[q].x;
+                if (ia != ca || ib != cb || tl != ctl || key < ckey) {
+                  const int2 f = pair_find(g, ia, ib);
+                  ca = ia; cb = ib; ctl = tl;
+                  cub = pair_first_t_after(g, f.x, f.x + f.y, tl);
+                  cs = pair_first_key_after(g, f.x, cub, key, strict_());
+                } else {
+                  // a few steps forward; fall back to a search for long jumps
+                  int steps_left = 4;
+                  while (cs < cub && steps_left-- > 0 &&
+                         (strict_() ? __ldg(&g.pair_rec[cs].y) : __ldg(&g.pair_rec[cs].x)) <= key) ++cs;
+                  if (steps_left < 0) cs = pair_first_key_after(g, cs, cub, key, strict_());
+                }
+                ckey = key;
+                cnt += (unsigned long long)(cub - cs);
+              }
+            }
           }
         } else {
-          push_children<l>(push, slot, rc, out, base, pos - 1, root);
+#pragma unroll
+          for (int q = 0; q < kScanWide; q++) {
+            bool push = false;
+            const int4 rc = rw[q];
+            if (pos < end) {
+              ++pos;
+              if (rc.z > tl) {
+                pos = end;
+              } else {
+                ++cand;
+                push = structural_ok(rc.y, want, nmc, m);
+              }
+            }
+            push_children<l>(push, slot, rc, out, base, pos - 1, root);
+            if (sm.nb[l + 1] >= 32) break;  // descend before the next push
+          }
         }
       }
     }
