@@ -29,6 +29,7 @@ FLAG_NO_STEAL = 4
 FLAG_NO_PAIR_INDEX = 8
 FLAG_PAIR_DIR = 16
 FLAG_CLOSING_SCAN = 32
+FLAG_NO_CLOSING_PRUNE = 64
 MAX_MOTIF_EDGES = 8
 
 # every symbol include/everest_b200.h declares

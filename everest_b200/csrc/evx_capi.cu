@@ -102,22 +102,24 @@ int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
 // pair run is the one the matched edge sits in: kQSamePair), and for a
 // closing edge whose pair changes with every partial match: one lookup per
 // partial match in the pair hash table (kQPairHash, the default) or, on
-// request, in the per-node pair directory (kQPairDir).
+// request, in the per-node pair directory (kQPairDir).  kQNoPrune turns off
+// the check of the closing edge's fixed endpoint before a task's scan.
 int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
+  const int np = (flags & EVX_FLAG_NO_CLOSING_PRUNE) ? kQNoPrune : 0;
   const int k = plan.k;
-  if (enumerate || (flags & EVX_FLAG_NO_PAIR_INDEX) || k < 2) return 0;
+  if (enumerate || (flags & EVX_FLAG_NO_PAIR_INDEX) || k < 2) return np;
   const int wl = plan.info[k - 2];
-  if (plan_kind(wl) != 2) return 0;
+  if (plan_kind(wl) != 2) return np;
   const int nm_prev = (k >= 3) ? plan_nm(plan.info[k - 3]) : 2;
-  if (plan_a(wl) < nm_prev && plan_b(wl) < nm_prev) return kQInlineLast;
+  if (plan_a(wl) < nm_prev && plan_b(wl) < nm_prev) return kQInlineLast | np;
   if (k >= 3) {
     const int wp = plan.info[k - 3];
-    if (plan_a(wp) == plan_a(wl) && plan_b(wp) == plan_b(wl)) return kQSamePair;
+    if (plan_a(wp) == plan_a(wl) && plan_b(wp) == plan_b(wl)) return kQSamePair | np;
     // the pair depends on the node the second-to-last edge maps
-    if (flags & EVX_FLAG_PAIR_DIR) return kQPairDir;
-    if (!(flags & EVX_FLAG_CLOSING_SCAN)) return kQPairHash;
+    if (flags & EVX_FLAG_PAIR_DIR) return kQPairDir | np;
+    if (!(flags & EVX_FLAG_CLOSING_SCAN)) return kQPairHash | np;
   }
-  return 0;
+  return np;
 }
 
 }  // namespace evx

@@ -75,6 +75,7 @@ constexpr int kQInlineLast = 2;  // closing last edge counted on the pair index
 constexpr int kQSamePair = 4;    // last edge repeats the previous edge's endpoints
 constexpr int kQPairDir = 8;     // last edge's pair found through the per-node pair directory
 constexpr int kQPairHash = 16;   // last edge's pair found through the pair hash table
+constexpr int kQNoPrune = 32;    // no closing-endpoint check before a task's scan
 struct QueryDesc {
   MotifPlan plan;
   int root_beg, root_end;  // root edge ids [beg, end)

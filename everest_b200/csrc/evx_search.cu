@@ -518,6 +518,30 @@ struct Searcher {
         cs = pair_first_key_after(g, f.x, cub, key, strict_());
         if (cs >= cub) pos = end;
       }
+      if (l == kr() - 3 && plan_kind(wl) == 2 && (la < nmc) != (lb < nmc) &&
+          !(qf & (kQInlineLast | kQSamePair | kQNoPrune)) && has && pos < end) {
+        // the closing edge has one endpoint mapped before this level, fixed
+        // for the task: when that node's list (out-list of a source, in-list
+        // of a destination) has no entry after the previous edge inside the
+        // window, no candidate of the task can close, so its scan is skipped
+        const bool fa = la < nmc;
+        const int x = sel(m, fa ? la : lb);
+        const int4 r = __ldg(g.node_rng + x);
+        int lo = fa ? r.x : r.z, hi = fa ? r.y : r.w;
+        const int4 *lst = fa ? g.out_rec : g.in_rec;
+        const int key = strict_() ? p.t : p.eid;
+        if (!strict_() && fa && p.src == x) lo = p.pop + 1;
+        else if (!strict_() && !fa && p.dst == x) lo = p.pip + 1;
+        else {
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            const int v = strict_() ? ld_t(lst + mid) : ld_eid(lst + mid);
+            if (v > key) hi = mid; else lo = mid + 1;
+          }
+          hi = fa ? r.y : r.w;
+        }
+        if (lo >= hi || ld_t(lst + lo) > tl) pos = end;
+      }
       while (true) {
         const unsigned act = __ballot_sync(kFull, pos < end);
         if (!inline_here) {

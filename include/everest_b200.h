@@ -50,6 +50,10 @@ extern "C" {
  * the per-node pair directory, or a scan of the shorter endpoint list. */
 #define EVX_FLAG_PAIR_DIR 16u
 #define EVX_FLAG_CLOSING_SCAN 32u
+/* Before scanning the candidates for the second-to-last edge, a search
+ * checks that the closing edge's fixed endpoint still has an edge inside the
+ * window (and skips the scan when not); this turns that check off. */
+#define EVX_FLAG_NO_CLOSING_PRUNE 64u
 
 typedef struct evx_graph evx_graph;   /* a graph resident on one device */
 typedef struct evx_worker evx_worker; /* per-device search worker */

@@ -62,6 +62,10 @@ def test_golden_small_graph_counts(golden, small_graphs, worker):
                 got3 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
                                  flags=capi.FLAG_PAIR_DIR)
                 assert got3 == c["count"], (gname, c["motif"], c["delta"], got3, "pair dir")
+            if n % 4 == 1:  # without the closing-endpoint check on a subset
+                got5 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
+                                 flags=capi.FLAG_NO_CLOSING_PRUNE)
+                assert got5 == c["count"], (gname, c["motif"], c["delta"], got5, "no prune")
             if n % 3 == 0:  # the scanned closing edge on a subset
                 got4 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
                                  flags=capi.FLAG_CLOSING_SCAN)
@@ -126,7 +130,8 @@ def test_random_tiny_vs_brute_force(worker):
         delta = int(rng.integers(0, 10))
         want = len(O.brute_force(u, v, t, mu, mv, delta))
         dg = device_graph(u, v, t)
-        for flags in (0, capi.FLAG_NO_STEAL, capi.FLAG_NO_PAIR_INDEX, capi.FLAG_PAIR_DIR, capi.FLAG_CLOSING_SCAN):
+        for flags in (0, capi.FLAG_NO_STEAL, capi.FLAG_NO_PAIR_INDEX, capi.FLAG_PAIR_DIR, capi.FLAG_CLOSING_SCAN,
+                      capi.FLAG_NO_CLOSING_PRUNE, capi.FLAG_NO_CLOSING_PRUNE | capi.FLAG_NO_PAIR_INDEX):
             assert gpu_count(worker, dg, mu, mv, delta, flags=flags) == want, (trial, pat, delta, flags)
         strict = len(O.brute_force(u, v, t, mu, mv, delta, strict_ts=True))
         assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS) == strict
