@@ -32,6 +32,8 @@ struct GraphView {
   const int2 *pair_loc;       // [e] = {position of e in pair_rec, end of its run}
   const int2 *pair_dir;       // [r] = {v, start} of run r, sorted by (u, v); [P] = sentinel
   const int *dir_off;         // [u] = first run of source u (V + 1 entries)
+  const unsigned long long *sig_out;  // [u] = OR of 1 << sig_bit(v) over u's out-neighbours v
+  const unsigned long long *sig_in;   // [v] = OR of 1 << sig_bit(u) over v's in-neighbours u
   unsigned long long pair_mask;
   int pair_max_probe;
   int num_edges;
@@ -50,6 +52,20 @@ __host__ __device__ inline unsigned long long pair_hash(unsigned long long x) {
   x *= 0x94d049bb133111ebull;
   x ^= x >> 31;
   return x;
+}
+
+// Bit of a node in the 64-bit neighbour signatures (Fibonacci hashing; a
+// different hash from the pair table's).
+__host__ __device__ inline int sig_bit(int x) {
+  return (int)(((unsigned long long)(unsigned)x * 0x9E3779B97F4A7C15ull) >> 58);
+}
+
+// False only when no u -> v edge exists: both signatures are small enough to
+// stay in L2, so most absent pairs are rejected without touching the pair
+// table.
+__device__ __forceinline__ bool pair_maybe(const GraphView &g, int u, int v) {
+  const unsigned long long so = __ldg(g.sig_out + u), si = __ldg(g.sig_in + v);
+  return ((so >> sig_bit(v)) & (si >> sig_bit(u)) & 1ull) != 0;
 }
 
 // Per-level search plan.  Level l (0-based) matches motif edge j = l + 1.
@@ -147,6 +163,7 @@ struct DeviceGraph {
   int2 *pair_loc = nullptr;
   int2 *pair_dir = nullptr;
   int *dir_off = nullptr;
+  unsigned long long *sig_out = nullptr, *sig_in = nullptr;
   unsigned long long pair_mask = 0;
   int pair_max_probe = 0;
   int64_t bytes = 0;
@@ -155,7 +172,7 @@ struct DeviceGraph {
     g.edges = edges; g.inpos = inpos; g.euid = euid; g.out_rec = out_rec; g.in_rec = in_rec;
     g.node_rng = node_rng;
     g.pair_tab = pair_tab; g.pair_rec = pair_rec; g.pair_loc = pair_loc; g.pair_mask = pair_mask;
-    g.pair_dir = pair_dir; g.dir_off = dir_off;
+    g.pair_dir = pair_dir; g.dir_off = dir_off; g.sig_out = sig_out; g.sig_in = sig_in;
     g.pair_max_probe = pair_max_probe;
     g.num_edges = (int)num_edges; g.num_vertices = (int)num_vertices;
     return g;

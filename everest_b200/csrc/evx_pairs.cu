@@ -61,6 +61,16 @@ __global__ void pair_dir_kernel(const unsigned long long *__restrict__ ukeys,
   }
 }
 
+// Neighbour signatures: one bit per neighbour (sig_bit) in each endpoint's word.
+__global__ void pair_sig_kernel(const int4 *__restrict__ edges, unsigned long long *__restrict__ sig_out,
+                                unsigned long long *__restrict__ sig_in, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int4 e = edges[i];
+    atomicOr(sig_out + e.x, 1ull << sig_bit(e.y));
+    atomicOr(sig_in + e.y, 1ull << sig_bit(e.x));
+  }
+}
+
 __global__ void pair_clear_kernel(int4 *__restrict__ tab, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -99,6 +109,14 @@ __global__ void pair_insert_kernel(const unsigned long long *__restrict__ ukeys,
 
 int build_pair_index(DeviceGraph &g, cudaStream_t s) {
   const int64_t E = g.num_edges;
+  {
+    const size_t vs = (size_t)(g.num_vertices > 0 ? g.num_vertices : 1);
+    EVX_CUDA(dev_alloc((void **)&g.sig_out, sizeof(unsigned long long) * vs, g.device, s));
+    EVX_CUDA(dev_alloc((void **)&g.sig_in, sizeof(unsigned long long) * vs, g.device, s));
+    EVX_CUDA(cudaMemsetAsync(g.sig_out, 0, sizeof(unsigned long long) * vs, s));
+    EVX_CUDA(cudaMemsetAsync(g.sig_in, 0, sizeof(unsigned long long) * vs, s));
+    g.bytes += (int64_t)(2 * sizeof(unsigned long long) * vs);
+  }
   if (E <= 0) {
     g.pair_mask = 0;
     g.pair_max_probe = 0;
@@ -155,6 +173,7 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     if (rc) goto cleanup;
     EVX_CUDA(cudaMemsetAsync(lens, 0, sizeof(int) * n, s));
     pair_keys_kernel<<<grid, block, 0, s>>>(g.edges, keys, vals, n);
+    pair_sig_kernel<<<grid, block, 0, s>>>(g.edges, g.sig_out, g.sig_in, n);
     cub::DeviceRadixSort::SortPairs(tmp, t1, keys, keys_sorted, vals, vals_sorted, n, 0, end_bit, s);
     cub::DeviceRunLengthEncode::Encode(tmp, t2, keys_sorted, ukeys, lens, ctr, n, s);
     // lens beyond the run count are never read by the scan's consumers; the

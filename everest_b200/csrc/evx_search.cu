@@ -50,6 +50,11 @@ constexpr int kWarps = kBlock / 32;
 #endif
 constexpr int kScanWide = EVX_SCAN_WIDE;
 
+// Check the neighbour signatures before a pair-table lookup.
+#ifndef EVX_PAIR_SIG
+#define EVX_PAIR_SIG 1
+#endif
+
 // resident blocks per SM the register budget aims for (deeper motifs keep
 // more per-level state live)
 #ifndef EVX_MINB3
@@ -380,8 +385,10 @@ struct Searcher {
       if (has) {
         const int w = plan.info[l];
         const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
-        const int2 f = pair_find(g, ia, ib);
-        cnt += (unsigned long long)pair_window(g, f.x, f.y, strict_() ? p.t : p.eid, tl, strict_());
+        if (EVX_PAIR_SIG == 0 || pair_maybe(g, ia, ib)) {
+          const int2 f = pair_find(g, ia, ib);
+          cnt += (unsigned long long)pair_window(g, f.x, f.y, strict_() ? p.t : p.eid, tl, strict_());
+        }
         ++cand;  // one lookup per task
       }
       return;
@@ -512,7 +519,7 @@ struct Searcher {
         // skipped
         const int ia = sel(m, la), ib = sel(m, lb);
         const int key = strict_() ? p.t : p.eid;
-        const int2 f = pair_find(g, ia, ib);
+        const int2 f = (EVX_PAIR_SIG == 0 || pair_maybe(g, ia, ib)) ? pair_find(g, ia, ib) : make_int2(0, 0);
         ca = ia; cb = ib; ctl = tl; ckey = key;
         cub = pair_first_t_after(g, f.x, f.x + f.y, tl);
         cs = pair_first_key_after(g, f.x, cub, key, strict_());
