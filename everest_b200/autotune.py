@@ -85,8 +85,10 @@ class Autotuner:
         own = worker is None
         w = worker or capi.Worker(self.device)
         E = graph.num_edges
-        S = min(E, self.sample_roots)
-        beg = max(0, (E - S) // 2)  # a middle slice: away from the empty start of the time range
+        # a middle slice (away from the empty start of the time range), or
+        # every root when sample_roots <= 0
+        S = E if self.sample_roots <= 0 else min(E, self.sample_roots)
+        beg = max(0, (E - S) // 2)
         best, best_ms, ref_count = None, float("inf"), None
         trials = []
         try:
