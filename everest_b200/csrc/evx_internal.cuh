@@ -30,6 +30,8 @@ struct GraphView {
   const int4 *pair_tab;
   const int2 *pair_rec;
   const int2 *pair_loc;       // [e] = {position of e in pair_rec, end of its run}
+  const int2 *rev_loc;        // [e] = {first position after e in the run of the reverse
+                              //        pair (v, u), end of that run}; {0, 0} when no v->u edge
   const int2 *pair_dir;       // [r] = {v, start} of run r, sorted by (u, v); [P] = sentinel
   const int *dir_off;         // [u] = first run of source u (V + 1 entries)
   const unsigned long long *sig_out;  // [u] = OR of 1 << sig_bit(v) over u's out-neighbours v
@@ -66,6 +68,21 @@ __host__ __device__ inline int sig_bit(int x) {
 __device__ __forceinline__ bool pair_maybe(const GraphView &g, int u, int v) {
   const unsigned long long so = __ldg(g.sig_out + u), si = __ldg(g.sig_in + v);
   return ((so >> sig_bit(v)) & (si >> sig_bit(u)) & 1ull) != 0;
+}
+
+// (start, len) of the run of u->v edges in pair_rec; len 0 when absent.  The
+// probe sequence stops at the longest one the table build used.
+__device__ __forceinline__ int2 pair_find(const GraphView &g, int u, int v) {
+  const unsigned long long key = pair_key(u, v);
+  unsigned long long h = pair_hash(key) & g.pair_mask;
+  for (int i = 0; i < g.pair_max_probe; i++) {
+    const int4 s = __ldg(g.pair_tab + h);
+    const unsigned long long k = ((unsigned long long)(unsigned)s.y << 32) | (unsigned)s.x;
+    if (k == key) return make_int2(s.z, s.w);
+    if (k == ~0ull) break;
+    h = (h + 1) & g.pair_mask;
+  }
+  return make_int2(0, 0);
 }
 
 // Per-level search plan.  Level l (0-based) matches motif edge j = l + 1.
@@ -161,6 +178,7 @@ struct DeviceGraph {
   int4 *pair_tab = nullptr;
   int2 *pair_rec = nullptr;
   int2 *pair_loc = nullptr;
+  int2 *rev_loc = nullptr;
   int2 *pair_dir = nullptr;
   int *dir_off = nullptr;
   unsigned long long *sig_out = nullptr, *sig_in = nullptr;
@@ -172,6 +190,7 @@ struct DeviceGraph {
     g.edges = edges; g.inpos = inpos; g.euid = euid; g.out_rec = out_rec; g.in_rec = in_rec;
     g.node_rng = node_rng;
     g.pair_tab = pair_tab; g.pair_rec = pair_rec; g.pair_loc = pair_loc; g.pair_mask = pair_mask;
+    g.rev_loc = rev_loc;
     g.pair_dir = pair_dir; g.dir_off = dir_off; g.sig_out = sig_out; g.sig_in = sig_in;
     g.pair_max_probe = pair_max_probe;
     g.num_edges = (int)num_edges; g.num_vertices = (int)num_vertices;

@@ -61,6 +61,22 @@ __global__ void pair_dir_kernel(const unsigned long long *__restrict__ ukeys,
   }
 }
 
+// rev[e] for e = (u, v): the entries of the reverse pair's run (v, u) after
+// e (edge id greater than e), as {first such position, end of the run};
+// {0, 0} when there is no v -> u edge.
+__global__ void rev_loc_kernel(const GraphView g, int2 *__restrict__ rev, int n) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int4 ed = g.edges[e];
+    const int2 f = pair_find(g, ed.y, ed.x);
+    int lo = f.x, hi = f.x + f.y;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (g.pair_rec[mid].x > e) hi = mid; else lo = mid + 1;
+    }
+    rev[e] = f.y > 0 ? make_int2(lo, f.x + f.y) : make_int2(0, 0);
+  }
+}
+
 // Neighbour signatures: one bit per neighbour (sig_bit) in each endpoint's word.
 __global__ void pair_sig_kernel(const int4 *__restrict__ edges, unsigned long long *__restrict__ sig_out,
                                 unsigned long long *__restrict__ sig_in, int n) {
@@ -123,6 +139,7 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     EVX_CUDA(dev_alloc((void **)&g.pair_tab, sizeof(int4), g.device, s));
     EVX_CUDA(dev_alloc((void **)&g.pair_rec, sizeof(int2), g.device, s));
     EVX_CUDA(dev_alloc((void **)&g.pair_loc, sizeof(int2), g.device, s));
+    EVX_CUDA(dev_alloc((void **)&g.rev_loc, sizeof(int2), g.device, s));
     EVX_CUDA(dev_alloc((void **)&g.pair_dir, sizeof(int2), g.device, s));
     EVX_CUDA(dev_alloc((void **)&g.dir_off, sizeof(int) * (size_t)(g.num_vertices + 1), g.device, s));
     EVX_CUDA(cudaMemsetAsync(g.pair_tab, 0xff, sizeof(int4), s));
@@ -132,7 +149,7 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
       EVX_CUDA(cudaMemcpyAsync(g.pair_dir, &sentinel, sizeof(int2), cudaMemcpyHostToDevice, s));
       EVX_CUDA(cudaStreamSynchronize(s));
     }
-    g.bytes += sizeof(int4) + 3 * sizeof(int2) + sizeof(int) * (g.num_vertices + 1);
+    g.bytes += sizeof(int4) + 4 * sizeof(int2) + sizeof(int) * (g.num_vertices + 1);
     return EVX_OK;
   }
   int sms = 148;
@@ -190,8 +207,9 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     cudaError_t e = dev_alloc((void **)&g.pair_tab, sizeof(int4) * (size_t)cap, g.device, s);
     if (e == cudaSuccess) e = dev_alloc((void **)&g.pair_rec, sizeof(int2) * (size_t)n, g.device, s);
     if (e == cudaSuccess) e = dev_alloc((void **)&g.pair_loc, sizeof(int2) * (size_t)n, g.device, s);
+    if (e == cudaSuccess) e = dev_alloc((void **)&g.rev_loc, sizeof(int2) * (size_t)n, g.device, s);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMalloc(pair index)"); goto cleanup; }
-    g.bytes += (int64_t)(sizeof(int4) * cap + 2 * sizeof(int2) * n);
+    g.bytes += (int64_t)(sizeof(int4) * cap + 3 * sizeof(int2) * n);
     EVX_CUDA(cudaMemsetAsync(ctr + 1, 0, 2 * sizeof(int), s));
     pair_clear_kernel<<<grid, block, 0, s>>>(g.pair_tab, cap);
     pair_rec_kernel<<<grid, block, 0, s>>>(vals_sorted, g.edges, g.pair_rec, n);
@@ -228,6 +246,8 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     EVX_CUDA(cudaStreamSynchronize(s));
     if (h[1]) { rc = fail(EVX_ERR_CUDA, "pair index insert overflow"); goto cleanup; }
     g.pair_max_probe = h[0];
+    rev_loc_kernel<<<grid, block, 0, s>>>(g.view(), g.rev_loc, n);
+    EVX_CUDA(cudaGetLastError());
   }
 cleanup:
   dev_free(keys, s);

@@ -80,21 +80,6 @@ __device__ __forceinline__ void put(int (&a)[N], int i, int v) {
 __device__ __forceinline__ int ld_eid(const int4 *p) { return __ldg(&p->x); }
 __device__ __forceinline__ int ld_t(const int4 *p) { return __ldg(&p->z); }
 
-// (start, len) of the run of u->v edges in pair_rec; len 0 when absent.  The
-// probe sequence stops at the longest one the table build used.
-__device__ __forceinline__ int2 pair_find(const GraphView &g, int u, int v) {
-  const unsigned long long key = pair_key(u, v);
-  unsigned long long h = pair_hash(key) & g.pair_mask;
-  for (int i = 0; i < g.pair_max_probe; i++) {
-    const int4 s = __ldg(g.pair_tab + h);
-    const unsigned long long k = ((unsigned long long)(unsigned)s.y << 32) | (unsigned)s.x;
-    if (k == key) return make_int2(s.z, s.w);
-    if (k == ~0ull) break;
-    h = (h + 1) & g.pair_mask;
-  }
-  return make_int2(0, 0);
-}
-
 // First index in [lo, hi) of pair_rec whose timestamp is greater than tl.
 __device__ __forceinline__ int pair_first_t_after(const GraphView &g, int lo, int hi, int tl) {
   while (lo < hi) {
@@ -517,12 +502,27 @@ struct Searcher {
         // run's entries after the previous edge inside the window once; when
         // there are none, no candidate of the task can close and its scan is
         // skipped
+        // (the previous edge's own pair, or its reverse, is located per edge
+        // without a table lookup)
         const int ia = sel(m, la), ib = sel(m, lb);
         const int key = strict_() ? p.t : p.eid;
-        const int2 f = (EVX_PAIR_SIG == 0 || pair_maybe(g, ia, ib)) ? pair_find(g, ia, ib) : make_int2(0, 0);
+        int lo, hi;
+        if (ia == p.src && ib == p.dst) {
+          const int2 pl = __ldg(g.pair_loc + p.eid);
+          lo = pl.x + 1; hi = pl.y;
+          if (strict_()) lo = pair_first_t_after(g, lo, hi, p.t);
+        } else if (ia == p.dst && ib == p.src) {
+          const int2 rl = __ldg(g.rev_loc + p.eid);
+          lo = rl.x; hi = rl.y;
+          if (strict_()) lo = pair_first_t_after(g, lo, hi, p.t);
+        } else {
+          const int2 f = (EVX_PAIR_SIG == 0 || pair_maybe(g, ia, ib)) ? pair_find(g, ia, ib) : make_int2(0, 0);
+          lo = pair_first_key_after(g, f.x, f.x + f.y, key, strict_());
+          hi = f.x + f.y;
+        }
         ca = ia; cb = ib; ctl = tl; ckey = key;
-        cub = pair_first_t_after(g, f.x, f.x + f.y, tl);
-        cs = pair_first_key_after(g, f.x, cub, key, strict_());
+        cs = lo;
+        cub = pair_gallop_t_after(g, lo, hi, tl);
         if (cs >= cub) pos = end;
       }
       if (l == kr() - 3 && plan_kind(wl) == 2 && (la < nmc) != (lb < nmc) &&
