@@ -317,6 +317,7 @@ int evx_graph_free(evx_graph *h) {
   dev_free(g.in_rec, s); dev_free(g.node_rng, s); dev_free(g.pair_tab, s); dev_free(g.pair_rec, s);
   dev_free(g.pair_loc, s); dev_free(g.pair_dir, s); dev_free(g.dir_off, s);
   dev_free(g.sig_out, s); dev_free(g.sig_in, s); dev_free(g.rev_loc, s);
+  dev_free(g.cross_out, s); dev_free(g.cross_in, s);
   cudaStreamSynchronize(s);
   delete h;
   return EVX_OK;

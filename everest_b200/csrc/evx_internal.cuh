@@ -30,6 +30,8 @@ struct GraphView {
   const int4 *pair_tab;
   const int2 *pair_rec;
   const int2 *pair_loc;       // [e] = {position of e in pair_rec, end of its run}
+  const int *cross_out;       // [e] = first position of out(v) holding an edge after e = (u, v)
+  const int *cross_in;        // [e] = first position of in(u) holding an edge after e = (u, v)
   const int2 *rev_loc;        // [e] = {first position after e in the run of the reverse
                               //        pair (v, u), end of that run}; {0, 0} when no v->u edge
   const int2 *pair_dir;       // [r] = {v, start} of run r, sorted by (u, v); [P] = sentinel
@@ -179,6 +181,7 @@ struct DeviceGraph {
   int2 *pair_rec = nullptr;
   int2 *pair_loc = nullptr;
   int2 *rev_loc = nullptr;
+  int *cross_out = nullptr, *cross_in = nullptr;
   int2 *pair_dir = nullptr;
   int *dir_off = nullptr;
   unsigned long long *sig_out = nullptr, *sig_in = nullptr;
@@ -190,7 +193,7 @@ struct DeviceGraph {
     g.edges = edges; g.inpos = inpos; g.euid = euid; g.out_rec = out_rec; g.in_rec = in_rec;
     g.node_rng = node_rng;
     g.pair_tab = pair_tab; g.pair_rec = pair_rec; g.pair_loc = pair_loc; g.pair_mask = pair_mask;
-    g.rev_loc = rev_loc;
+    g.rev_loc = rev_loc; g.cross_out = cross_out; g.cross_in = cross_in;
     g.pair_dir = pair_dir; g.dir_off = dir_off; g.sig_out = sig_out; g.sig_in = sig_in;
     g.pair_max_probe = pair_max_probe;
     g.num_edges = (int)num_edges; g.num_vertices = (int)num_vertices;

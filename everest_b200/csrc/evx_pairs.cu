@@ -77,6 +77,30 @@ __global__ void rev_loc_kernel(const GraphView g, int2 *__restrict__ rev, int n)
   }
 }
 
+// Cross-list starts: for e = (u, v), the first position of out(v) and of
+// in(u) whose edge comes after e (the two endpoint lists e is not in), so
+// a search that extends e from either endpoint starts without a binary
+// search.
+__global__ void cross_pos_kernel(const int4 *__restrict__ edges, const int4 *__restrict__ node_rng,
+                                 const int4 *__restrict__ out_rec, const int4 *__restrict__ in_rec,
+                                 int *__restrict__ cross_out, int *__restrict__ cross_in, int n) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const int4 ed = edges[e];
+    int lo = node_rng[ed.y].x, hi = node_rng[ed.y].y;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (out_rec[mid].x > e) hi = mid; else lo = mid + 1;
+    }
+    cross_out[e] = lo;
+    lo = node_rng[ed.x].z; hi = node_rng[ed.x].w;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (in_rec[mid].x > e) hi = mid; else lo = mid + 1;
+    }
+    cross_in[e] = lo;
+  }
+}
+
 // Neighbour signatures: one bit per neighbour (sig_bit) in each endpoint's word.
 __global__ void pair_sig_kernel(const int4 *__restrict__ edges, unsigned long long *__restrict__ sig_out,
                                 unsigned long long *__restrict__ sig_in, int n) {
@@ -140,6 +164,8 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     EVX_CUDA(dev_alloc((void **)&g.pair_rec, sizeof(int2), g.device, s));
     EVX_CUDA(dev_alloc((void **)&g.pair_loc, sizeof(int2), g.device, s));
     EVX_CUDA(dev_alloc((void **)&g.rev_loc, sizeof(int2), g.device, s));
+    EVX_CUDA(dev_alloc((void **)&g.cross_out, sizeof(int), g.device, s));
+    EVX_CUDA(dev_alloc((void **)&g.cross_in, sizeof(int), g.device, s));
     EVX_CUDA(dev_alloc((void **)&g.pair_dir, sizeof(int2), g.device, s));
     EVX_CUDA(dev_alloc((void **)&g.dir_off, sizeof(int) * (size_t)(g.num_vertices + 1), g.device, s));
     EVX_CUDA(cudaMemsetAsync(g.pair_tab, 0xff, sizeof(int4), s));
@@ -149,7 +175,7 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
       EVX_CUDA(cudaMemcpyAsync(g.pair_dir, &sentinel, sizeof(int2), cudaMemcpyHostToDevice, s));
       EVX_CUDA(cudaStreamSynchronize(s));
     }
-    g.bytes += sizeof(int4) + 4 * sizeof(int2) + sizeof(int) * (g.num_vertices + 1);
+    g.bytes += sizeof(int4) + 5 * sizeof(int2) + sizeof(int) * (g.num_vertices + 1);
     return EVX_OK;
   }
   int sms = 148;
@@ -208,8 +234,10 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     if (e == cudaSuccess) e = dev_alloc((void **)&g.pair_rec, sizeof(int2) * (size_t)n, g.device, s);
     if (e == cudaSuccess) e = dev_alloc((void **)&g.pair_loc, sizeof(int2) * (size_t)n, g.device, s);
     if (e == cudaSuccess) e = dev_alloc((void **)&g.rev_loc, sizeof(int2) * (size_t)n, g.device, s);
+    if (e == cudaSuccess) e = dev_alloc((void **)&g.cross_out, sizeof(int) * (size_t)n, g.device, s);
+    if (e == cudaSuccess) e = dev_alloc((void **)&g.cross_in, sizeof(int) * (size_t)n, g.device, s);
     if (e != cudaSuccess) { rc = cuda_fail(e, "cudaMalloc(pair index)"); goto cleanup; }
-    g.bytes += (int64_t)(sizeof(int4) * cap + 3 * sizeof(int2) * n);
+    g.bytes += (int64_t)(sizeof(int4) * cap + 4 * sizeof(int2) * n);
     EVX_CUDA(cudaMemsetAsync(ctr + 1, 0, 2 * sizeof(int), s));
     pair_clear_kernel<<<grid, block, 0, s>>>(g.pair_tab, cap);
     pair_rec_kernel<<<grid, block, 0, s>>>(vals_sorted, g.edges, g.pair_rec, n);
@@ -247,6 +275,7 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     if (h[1]) { rc = fail(EVX_ERR_CUDA, "pair index insert overflow"); goto cleanup; }
     g.pair_max_probe = h[0];
     rev_loc_kernel<<<grid, block, 0, s>>>(g.view(), g.rev_loc, n);
+    cross_pos_kernel<<<grid, block, 0, s>>>(g.edges, g.node_rng, g.out_rec, g.in_rec, g.cross_out, g.cross_in, n);
     EVX_CUDA(cudaGetLastError());
   }
 cleanup:

@@ -283,6 +283,16 @@ struct Searcher {
     }
   }
 
+  // First position of out(x) / in(x) after the previous edge p when it is
+  // known without a search (p is in the list, or p's other endpoint is x),
+  // else -1.
+  __device__ __forceinline__ int out_start(const Prev &p, int x) const {
+    return p.src == x ? p.pop + 1 : (p.dst == x ? __ldg(g.cross_out + p.eid) : -1);
+  }
+  __device__ __forceinline__ int in_start(const Prev &p, int x) const {
+    return p.dst == x ? p.pip + 1 : (p.src == x ? __ldg(g.cross_in + p.eid) : -1);
+  }
+
   __device__ __forceinline__ bool structural_ok(int node, int want, int nmc, const int (&m)[N]) const {
     if (want >= 0) return node == want;
     bool ok = true;
@@ -409,19 +419,19 @@ struct Searcher {
         const int4 ro = __ldg(g.node_rng + ia);
         if (ri.w - ri.z < ro.y - ro.x) {
           out = false; base = ib; want = ia; lo = ri.z; hi = ri.w;
-          sc = (p.dst == ib) ? p.pip + 1 : -1;
+          sc = in_start(p, ib);
         } else {
           out = true; base = ia; want = ib; lo = ro.x; hi = ro.y;
-          sc = (p.src == ia) ? p.pop + 1 : -1;
+          sc = out_start(p, ia);
         }
       } else if (kind == 1) {
         const int4 r = __ldg(g.node_rng + ia);
         out = true; base = ia; lo = r.x; hi = r.y;
-        sc = (p.src == ia) ? p.pop + 1 : -1;
+        sc = out_start(p, ia);
       } else {
         const int4 r = __ldg(g.node_rng + ib);
         out = false; base = ib; lo = r.z; hi = r.w;
-        sc = (p.dst == ib) ? p.pip + 1 : -1;
+        sc = in_start(p, ib);
       }
       end = hi;
       if (!strict_() && sc >= 0) {
@@ -537,8 +547,8 @@ struct Searcher {
         int lo = fa ? r.x : r.z, hi = fa ? r.y : r.w;
         const int4 *lst = fa ? g.out_rec : g.in_rec;
         const int key = strict_() ? p.t : p.eid;
-        if (!strict_() && fa && p.src == x) lo = p.pop + 1;
-        else if (!strict_() && !fa && p.dst == x) lo = p.pip + 1;
+        const int known = strict_() ? -1 : (fa ? out_start(p, x) : in_start(p, x));
+        if (known >= 0) lo = known;
         else {
           while (lo < hi) {
             const int mid = (lo + hi) >> 1;
