@@ -99,7 +99,8 @@ int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
 // mode) for a closing last edge: when it closes on two nodes mapped before
 // the second-to-last edge (its pair is fixed per partial match:
 // kQInlineLast), when it repeats the second-to-last edge's endpoints (its
-// pair run is the one the matched edge sits in: kQSamePair), and for a
+// pair run is the one the matched edge sits in: kQSamePair; when it reverses
+// them, the reverse pair's run located per edge: kQRevPair), and for a
 // closing edge whose pair changes with every partial match: one lookup per
 // partial match in the pair hash table (kQPairHash, the default) or, on
 // request, in the per-node pair directory (kQPairDir).  kQNoPrune turns off
@@ -115,6 +116,7 @@ int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
   if (k >= 3) {
     const int wp = plan.info[k - 3];
     if (plan_a(wp) == plan_a(wl) && plan_b(wp) == plan_b(wl)) return kQSamePair | np;
+    if (plan_a(wp) == plan_b(wl) && plan_b(wp) == plan_a(wl)) return kQRevPair | np;
     // the pair depends on the node the second-to-last edge maps
     if (flags & EVX_FLAG_PAIR_DIR) return kQPairDir | np;
     if (!(flags & EVX_FLAG_CLOSING_SCAN)) return kQPairHash | np;

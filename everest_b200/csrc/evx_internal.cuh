@@ -111,6 +111,7 @@ constexpr int kQSamePair = 4;    // last edge repeats the previous edge's endpoi
 constexpr int kQPairDir = 8;     // last edge's pair found through the per-node pair directory
 constexpr int kQPairHash = 16;   // last edge's pair found through the pair hash table
 constexpr int kQNoPrune = 32;    // no closing-endpoint check before a task's scan
+constexpr int kQRevPair = 64;    // last edge reverses the previous edge's endpoints
 struct QueryDesc {
   MotifPlan plan;
   int root_beg, root_end;  // root edge ids [beg, end)

@@ -503,7 +503,7 @@ struct Searcher {
       // --------------------------------- scan, queue children, descend ----
       // The level before the last one counts a closing last edge inline by
       // range arithmetic on the pair index (count mode only).
-      const bool inline_here = (l == kr() - 3) && !ENUM && (qf & (kQInlineLast | kQSamePair));
+      const bool inline_here = (l == kr() - 3) && !ENUM && (qf & (kQInlineLast | kQSamePair | kQRevPair));
       const int wl = plan.info[kr() - 2];
       const int la = plan_a(wl), lb = plan_b(wl);
       int ca = -1, cb = -1, ctl = 0, cs = 0, cub = 0, ckey = 0;  // this lane's pair cursor
@@ -536,7 +536,7 @@ struct Searcher {
         if (cs >= cub) pos = end;
       }
       if (l == kr() - 3 && plan_kind(wl) == 2 && (la < nmc) != (lb < nmc) &&
-          !(qf & (kQInlineLast | kQSamePair | kQNoPrune)) && has && pos < end) {
+          !(qf & (kQInlineLast | kQNoPrune)) && has && pos < end) {
         // the closing edge has one endpoint mapped before this level, fixed
         // for the task: when that node's list (out-list of a source, in-list
         // of a destination) has no entry after the previous edge inside the
@@ -613,17 +613,19 @@ struct Searcher {
               }
             }
           }
-          if (qf & kQSamePair) {
-            // the last edge repeats the matched edge's endpoints: count the
-            // rest of that edge's own pair run inside the window
+          if (qf & (kQSamePair | kQRevPair)) {
+            // the last edge repeats the matched edge's endpoints (or reverses
+            // them): count the entries of that edge's own pair run (or of the
+            // reverse pair's run) after the edge and inside the window
+            const bool rev = (qf & kQRevPair) != 0;
             int2 pl[kScanWide];
 #pragma unroll
             for (int q = 0; q < kScanWide; q++)
-              pl[q] = ok[q] ? __ldg(g.pair_loc + rw[q].x) : make_int2(0, 0);
+              pl[q] = ok[q] ? __ldg((rev ? g.rev_loc : g.pair_loc) + rw[q].x) : make_int2(0, 0);
 #pragma unroll
             for (int q = 0; q < kScanWide; q++) {
               if (ok[q]) {
-                int lo = pl[q].x + 1;
+                int lo = rev ? pl[q].x : pl[q].x + 1;
                 if (strict_()) lo = pair_first_t_after(g, lo, pl[q].y, rw[q].z);
                 cnt += (unsigned long long)(pair_gallop_t_after(g, lo, pl[q].y, tl) - lo);
               }
