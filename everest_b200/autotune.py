@@ -37,6 +37,7 @@ CANDIDATES = [
     {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_CLOSING_SCAN},
     {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_CLOSING_SCAN},
     {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_NO_CLOSING_PRUNE},
+    {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_NEW_SCAN},
     {"blocks_per_sm": 4, "steal_interval": 16, "min_split": 2, "flags": 0},
 ]
 BATCH_TILES = (64, 128, 256, 512)

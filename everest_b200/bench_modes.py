@@ -118,7 +118,8 @@ def run_batch(args) -> int:
                                    f"on 2-4 nodes, delta cycling 3600/86400/604800, roots = a random window "
                                    f"of {window} edges per query", "tile_roots": tile,
                        "work_limit": limit, "cuda_graph": True},
-            "one_at_a_time": {"value": n / t_seq, "unit": "queries/s", "ms_per_step": t_seq * 1e3},
+            "one_at_a_time": {"value": n / t_seq, "unit": "queries/s", "ms_per_step": t_seq * 1e3,
+                              "limited_ms": float(sum(svc[i] for i, r in enumerate(seq) if r[1]) * 1e3)},
             "speedup": t_seq / t_bat, "batched_device_ms": float(np.mean(dev_ms)),
             "matches": matches, "limited_queries": int(sum(lim for _, lim, _ in seq)),
             "results_equal": True}
@@ -189,6 +190,9 @@ def run_serve(args) -> int:
                                    f"[1e4, 1e6]), roots = a random window of {window} edges per query",
                        "work_limit": limit, "poisson_rate_qps": rate},
             "one_at_a_time": {"value": seq_qps, "unit": "queries/s",
+                              "service_s": {"count": float(sum(svc[i] for i in cnt)),
+                                            "enumerate": float(sum(svc[i] for i, q in enumerate(qs) if q["cap"])),
+                                            "limited": float(sum(svc[i] for i, r in enumerate(seq) if r[1]))},
                               "service_p50_ms": _pct(svc, 50), "service_p99_ms": _pct(svc, 99),
                               "poisson_p50_ms": _pct(seq_lat, 50), "poisson_p99_ms": _pct(seq_lat, 99),
                               "poisson_p999_ms": _pct(seq_lat, 99.9)},

@@ -104,13 +104,15 @@ int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
 // closing edge whose pair changes with every partial match: one lookup per
 // partial match in the pair hash table (kQPairHash, the default) or, on
 // request, in the per-node pair directory (kQPairDir).  kQNoPrune turns off
-// the check of the closing edge's fixed endpoint before a task's scan.
+// the check of the closing edge's fixed endpoint before a task's scan.  A last
+// edge that maps a new node is scanned, and past the first step of a window
+// the rest is counted by range arithmetic (kQNewArith) unless asked not to.
 int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
   const int np = (flags & EVX_FLAG_NO_CLOSING_PRUNE) ? kQNoPrune : 0;
   const int k = plan.k;
   if (enumerate || (flags & EVX_FLAG_NO_PAIR_INDEX) || k < 2) return np;
   const int wl = plan.info[k - 2];
-  if (plan_kind(wl) != 2) return np;
+  if (plan_kind(wl) != 2) return np | ((flags & EVX_FLAG_NEW_SCAN) ? 0 : kQNewArith);
   const int nm_prev = (k >= 3) ? plan_nm(plan.info[k - 3]) : 2;
   if (plan_a(wl) < nm_prev && plan_b(wl) < nm_prev) return kQInlineLast | np;
   if (k >= 3) {

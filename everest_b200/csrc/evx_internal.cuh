@@ -112,6 +112,7 @@ constexpr int kQPairDir = 8;     // last edge's pair found through the per-node 
 constexpr int kQPairHash = 16;   // last edge's pair found through the pair hash table
 constexpr int kQNoPrune = 32;    // no closing-endpoint check before a task's scan
 constexpr int kQRevPair = 64;    // last edge reverses the previous edge's endpoints
+constexpr int kQNewArith = 128;  // a new-node last edge's long windows counted by range arithmetic
 struct QueryDesc {
   MotifPlan plan;
   int root_beg, root_end;  // root edge ids [beg, end)

@@ -163,6 +163,39 @@ __device__ __forceinline__ int pair_window(const GraphView &g, int start, int le
   return c - a;
 }
 
+// First position in [lo, hi) of an adjacency list whose timestamp is
+// greater than tl, galloping up from lo (windows are usually short).
+__device__ __forceinline__ int list_first_t_after(const int4 *lst, int lo, int hi, int tl) {
+  int step = 1;
+  while (lo < hi) {
+    const int probe = min(lo + step - 1, hi - 1);
+    if (ld_t(lst + probe) > tl) { hi = probe; break; }
+    lo = probe + 1;
+    step <<= 1;
+  }
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ld_t(lst + mid) > tl) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+// Entries of the pair run [start, start + len) whose edge id lies in [klo, khi].
+__device__ __forceinline__ int pair_count_eids(const GraphView &g, int start, int len, int klo, int khi) {
+  if (len <= 0) return 0;
+  int a = start, b = start + len;
+  while (a < b) {
+    const int mid = (a + b) >> 1;
+    if (__ldg(&g.pair_rec[mid].x) >= klo) b = mid; else a = mid + 1;
+  }
+  int c = a, d = start + len;
+  while (c < d) {
+    const int mid = (c + d) >> 1;
+    if (__ldg(&g.pair_rec[mid].x) > khi) d = mid; else c = mid + 1;
+  }
+  return c - a;
+}
+
 // Per-warp shared state.
 //   root[r]           = {u, v, tl, e0} of the batch's root on lane r
 //   task[l-1][s][0/1] = {parent, src, dst, eid}, {t, pos in out_rec, pos in in_rec, root}
@@ -485,6 +518,33 @@ struct Searcher {
                   if (ENUM) { emit = true; last_eid = rr[q].x; }
                 }
               }
+            }
+          }
+          if constexpr (!ENUM) {
+            if (want < 0 && pos < end && (qf & kQNewArith)) {
+              // a last edge that maps a new node, and the window goes on past
+              // this step: the rest of the window counts every record except
+              // those whose other endpoint is already mapped, i.e. the
+              // entries of the pairs (base, m_j) (or (m_j, base)) inside the
+              // same edge-id range
+              const int wend = list_first_t_after(lst, pos, end, tl);
+              if (wend > pos) {
+                const int klo = ld_eid(lst + pos), khi = ld_eid(lst + wend - 1);
+                int sub = 0;
+#pragma unroll
+                for (int j = 0; j < N; j++) {
+                  if (j < nmc) {
+                    const int a_ = out ? base : m[j], b_ = out ? m[j] : base;
+                    if (pair_maybe(g, a_, b_)) {
+                      const int2 f = pair_find(g, a_, b_);
+                      sub += pair_count_eids(g, f.x, f.y, klo, khi);
+                    }
+                  }
+                }
+                cnt += (unsigned long long)(wend - pos - sub);
+                cand += (unsigned)(wend - pos);  // the meter covers counted records too
+              }
+              pos = end;
             }
           }
         }

@@ -54,6 +54,11 @@ extern "C" {
  * checks that the closing edge's fixed endpoint still has an edge inside the
  * window (and skips the scan when not); this turns that check off. */
 #define EVX_FLAG_NO_CLOSING_PRUNE 64u
+/* A last edge that maps a new node is scanned four records per lane per
+ * step; when its window goes on past that, the rest is counted by range
+ * arithmetic (window length minus the entries of the pairs to nodes already
+ * mapped).  This keeps the scan instead. */
+#define EVX_FLAG_NEW_SCAN 128u
 
 typedef struct evx_graph evx_graph;   /* a graph resident on one device */
 typedef struct evx_worker evx_worker; /* per-device search worker */
