@@ -163,6 +163,13 @@ __device__ __forceinline__ int pair_window(const GraphView &g, int start, int le
   return c - a;
 }
 
+// A new-node last edge's window is counted by range arithmetic when more than
+// this many records per already-mapped node remain (one pair probe each).
+#ifndef EVX_ARITH_RECS
+#define EVX_ARITH_RECS 8
+#endif
+constexpr int kArithRecs = EVX_ARITH_RECS;
+
 // First position in [lo, hi) of an adjacency list whose timestamp is
 // greater than tl, galloping up from lo (windows are usually short).
 __device__ __forceinline__ int list_first_t_after(const int4 *lst, int lo, int hi, int tl) {
@@ -492,6 +499,7 @@ struct Searcher {
     int steps = 0;
     if (l == kr() - 2 || l == L - 1) {
       // ------------------------------------------------ last level ----
+      bool arith = true;  // the range-arithmetic check is still to be made
       while (true) {
         const unsigned act = __ballot_sync(kFull, pos < end);
         if (!act) break;
@@ -521,14 +529,18 @@ struct Searcher {
             }
           }
           if constexpr (!ENUM) {
-            if (want < 0 && pos < end && (qf & kQNewArith)) {
+            if (want < 0 && pos < end && arith && (qf & kQNewArith)) {
               // a last edge that maps a new node, and the window goes on past
-              // this step: the rest of the window counts every record except
-              // those whose other endpoint is already mapped, i.e. the
-              // entries of the pairs (base, m_j) (or (m_j, base)) inside the
-              // same edge-id range
+              // this step: when the rest of the window is long, it counts
+              // every record except those whose other endpoint is already
+              // mapped, i.e. the entries of the pairs (base, m_j) (or
+              // (m_j, base)) inside the same edge-id range; a short rest is
+              // scanned (each pair costs a table probe)
+              arith = false;
               const int wend = list_first_t_after(lst, pos, end, tl);
-              if (wend > pos) {
+              if (wend - pos <= kArithRecs * nmc) {
+                end = wend;
+              } else {
                 const int klo = ld_eid(lst + pos), khi = ld_eid(lst + wend - 1);
                 int sub = 0;
 #pragma unroll
@@ -543,8 +555,8 @@ struct Searcher {
                 }
                 cnt += (unsigned long long)(wend - pos - sub);
                 cand += (unsigned)(wend - pos);  // the meter covers counted records too
+                pos = end;
               }
-              pos = end;
             }
           }
         }
