@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--queries", type=int, default=0, help="batch/serve: number of queries")
     ap.add_argument("--window", type=int, default=0,
                     help="batch/serve: roots per query (a random time window of the edge list)")
+    ap.add_argument("--serve-slots", default="64,2,2,2",
+                    help="serve: max queries per batch, batches in flight, enumeration slots, "
+                         "blocks per SM of an enumeration (0 = all)")
     ap.add_argument("--limit", type=float, default=1e9,
                     help="batch/serve: work limit per query, in adjacency records examined inside "
                          "their time windows (stopped queries are flagged in both arms)")

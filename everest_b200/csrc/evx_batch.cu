@@ -36,7 +36,7 @@ struct evx_batch {
   unsigned long long limit = 0;  // work limit per query (0 = none)
   // captured launch and the shape it was captured for
   cudaGraphExec_t exec = nullptr;
-  int exec_nq = -1, exec_kmax = -1, exec_tiles = -1, exec_grid = -1, exec_tile_roots = -1;
+  int exec_nq = -1, exec_kmax = -1, exec_tiles = -1, exec_grid = -1, exec_tile_roots = -1, exec_uniform = -1;
   unsigned long long exec_limit = 0;
   const evx_graph *exec_graph = nullptr;
   bool launched = false;
@@ -52,7 +52,7 @@ void drop_exec(evx_batch *b) {
   b->exec_nq = -1;
 }
 
-int enqueue(evx_batch *b, int nq, int kmax, int total_tiles, int grid) {
+int enqueue(evx_batch *b, int nq, int kmax, bool uniform, int total_tiles, int grid) {
   int *cursor = reinterpret_cast<int *>(b->counts_d + b->max_q);
   EVX_CUDA(cudaMemcpyAsync(b->table_d, b->table_h, sizeof(QueryDesc) * (size_t)nq, cudaMemcpyHostToDevice,
                            b->stream));
@@ -67,7 +67,7 @@ int enqueue(evx_batch *b, int nq, int kmax, int total_tiles, int grid) {
   la.limit = b->limit;
   la.meter = b->counts_d + b->max_q + 1;
   if (total_tiles > 0) {
-    int rc = launch_table(b->graph->g.view(), b->table_h[0], la, kmax, grid, b->stream);
+    int rc = launch_table(b->graph->g.view(), b->table_h[0], la, kmax, uniform, grid, b->stream);
     if (rc) return rc;
     EVX_CUDA(cudaGetLastError());
   }
@@ -215,26 +215,29 @@ int evx_batch_launch(evx_batch *b) {
     if (q.plan.k > kmax) kmax = q.plan.k;
     b->table_h[i] = q;
   }
+  bool uniform = true;
+  for (int i = 0; i < nq; i++) uniform = uniform && b->table_h[i].plan.k == kmax;
   int bps = b->blocks_per_sm;
   if (bps <= 0) {
-    int rc = table_occupancy(kmax, &bps);  // also sets the kernel attributes before any capture
+    int rc = table_occupancy(kmax, uniform, &bps);  // also sets the kernel attributes before any capture
     if (rc) return rc;
     if (bps < 1) bps = 1;
   } else {
     int dummy = 0;
-    int rc = table_occupancy(kmax, &dummy);
+    int rc = table_occupancy(kmax, uniform, &dummy);
     if (rc) return rc;
   }
   const int grid = bps * b->num_sms;
   EVX_CUDA(cudaEventRecord(b->ev0, b->stream));
   if (b->use_graph) {
     if (!b->exec || b->exec_nq != nq || b->exec_kmax != kmax || b->exec_tiles != tiles ||
+        b->exec_uniform != (int)uniform ||
         b->exec_grid != grid || b->exec_tile_roots != b->tile_roots || b->exec_graph != b->graph ||
         b->exec_limit != b->limit) {
       drop_exec(b);
       cudaGraph_t graph = nullptr;
       EVX_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-      int rc = enqueue(b, nq, kmax, tiles, grid);
+      int rc = enqueue(b, nq, kmax, uniform, tiles, grid);
       cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
       if (rc) {
         if (graph) cudaGraphDestroy(graph);
@@ -245,11 +248,12 @@ int evx_batch_launch(evx_batch *b) {
       cudaGraphDestroy(graph);
       if (e != cudaSuccess) { b->exec = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
       b->exec_nq = nq; b->exec_kmax = kmax; b->exec_tiles = tiles; b->exec_grid = grid;
+      b->exec_uniform = (int)uniform;
       b->exec_tile_roots = b->tile_roots; b->exec_graph = b->graph; b->exec_limit = b->limit;
     }
     EVX_CUDA(cudaGraphLaunch(b->exec, b->stream));
   } else {
-    int rc = enqueue(b, nq, kmax, tiles, grid);
+    int rc = enqueue(b, nq, kmax, uniform, tiles, grid);
     if (rc) return rc;
   }
   EVX_CUDA(cudaEventRecord(b->ev1, b->stream));

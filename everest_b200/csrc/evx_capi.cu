@@ -371,9 +371,9 @@ int evx_worker_create(int device, void *stream, evx_worker **out) {
 int evx_worker_destroy(evx_worker *w) {
   if (!w) return EVX_OK;
   cudaSetDevice(w->device);
+  if (w->rows_d && w->stream) dev_free(w->rows_d, w->stream);
   if (w->stream) cudaStreamSynchronize(w->stream);
   cudaFree(w->state_d);
-  cudaFree(w->rows_d);
   if (w->count_h) cudaFreeHost(w->count_h);
   if (w->ev0) cudaEventDestroy(w->ev0);
   if (w->ev1) cudaEventDestroy(w->ev1);
@@ -435,9 +435,13 @@ int evx_worker_take(evx_worker *w, const evx_graph *gh, int k, const int *mu, co
       if (bytes + reserve > fr)
         return fail(EVX_ERR_NOMEM, "enumeration buffer of " + std::to_string(bytes) +
                                        " bytes not admitted (free " + std::to_string(fr) + ")");
-      if (w->rows_d) { cudaFree(w->rows_d); w->rows_d = nullptr; w->rows_cap = 0; }
-      EVX_CUDA(cudaMalloc(&w->rows_d, bytes));
-      w->rows_cap = need;
+      // stream-ordered pool memory: no device-wide synchronisation, so a
+      // serving loop's other streams keep running while a buffer grows
+      int64_t grow = need;
+      if (2 * w->rows_cap > grow && (size_t)(2 * w->rows_cap) * sizeof(int) + reserve <= fr) grow = 2 * w->rows_cap;
+      if (w->rows_d) { dev_free(w->rows_d, w->stream); w->rows_d = nullptr; w->rows_cap = 0; }
+      EVX_CUDA(dev_alloc((void **)&w->rows_d, (size_t)grow * sizeof(int), w->device, w->stream));
+      w->rows_cap = grow;
     }
   }
   w->view = g.view();

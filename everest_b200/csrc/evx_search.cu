@@ -272,8 +272,8 @@ struct Searcher {
   // the one record past a window that ends each scan, nor binary-search
   // probes): every such record is examined exactly once however the scans
   // are split between lanes, so the meter's final value is fixed by the
-  // graph and the query.  Lanes add to it once one holds 512 records (so
-  // the records not yet added stay below 512 x the lanes of the grid); the
+  // graph and the query.  Lanes add to it once one holds 64 records (so
+  // the records not yet added stay below 64 x the lanes of the grid); the
   // total returned by that add is what is compared, so a query is stopped
   // only once its final meter is known to exceed the limit.
   __device__ __forceinline__ bool halted() {
@@ -282,7 +282,7 @@ struct Searcher {
       if (!ea.exact_total && *(volatile int *)ea.stop != 0) return true;
     }
     if (!la.limit) return false;
-    if (!__any_sync(kFull, cand >= 512u)) return false;
+    if (!__any_sync(kFull, cand >= 64u)) return false;
     return meter_add() > la.limit;
   }
 
@@ -1031,11 +1031,15 @@ int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &a
   EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
 }
 
-int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int kmax, int grid,
-                 cudaStream_t stream) {
+int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int kmax, bool uniform,
+                 int grid, cudaStream_t stream) {
   const int k = kmax;
+  const bool enumerate = false;
   EnumArgs ea;
   memset(&ea, 0, sizeof(ea));
+  // every query of size kmax: the exact-size kernel (its levels are
+  // compile-time, like a single query's)
+  if (uniform) EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
   EVX_T_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
 }
 
@@ -1044,8 +1048,10 @@ int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm) {
   EVX_K_DISPATCH(occ_k, blocks_per_sm)
 }
 
-int table_occupancy(int kmax, int *blocks_per_sm) {
+int table_occupancy(int kmax, bool uniform, int *blocks_per_sm) {
   const int k = kmax;
+  const bool enumerate = false;
+  if (uniform) EVX_K_DISPATCH(occ_k, blocks_per_sm)
   EVX_T_DISPATCH(occ_k, blocks_per_sm)
 }
 

@@ -62,7 +62,8 @@ class Result:
 class Server:
     def __init__(self, device: int = 0, max_batch: int = 64, inflight_batches: int = 2,
                  enum_slots: int = 2, mem_reserve: int = 1 << 30, idle_sleep_s: float = 50e-6,
-                 backend=None, limit: int = 0):
+                 backend=None, limit: int = 0, use_graph: bool = False, tile_roots: int = 64,
+                 enum_blocks_per_sm: int = 2):
         # backend: the module providing Batch, Worker, DeviceGraph and
         # device_mem_info (the C-ABI binding; tests substitute a fake)
         self.be = backend if backend is not None else capi
@@ -78,16 +79,33 @@ class Server:
         self.cv = threading.Condition(self.lock)
         self.limit = int(limit)
         self.batches = [capi_.Batch(device, max_batch) for _ in range(inflight_batches)]
-        if self.limit:
-            for b in self.batches:
+        for b in self.batches:
+            if self.limit:
                 b.set_limit(self.limit)
+            # served batches change shape from one launch to the next, so a
+            # captured CUDA graph would be re-instantiated almost every time:
+            # launch directly unless asked otherwise.  Small tiles: one heavy
+            # query of a batch then spreads over many warps instead of
+            # holding the whole batch back on a few
+            if hasattr(b, "set_tuning"):
+                b.set_tuning(tile_roots=tile_roots, use_graph=use_graph)
         self.batch_reqs: List[Optional[List[Request]]] = [None] * inflight_batches
         self.enum_workers = [capi_.Worker(device) for _ in range(enum_slots)]
-        if self.limit:
-            for w in self.enum_workers:
+        for w in self.enum_workers:
+            if self.limit:
                 w.set_limit(self.limit)
+            # an enumeration's kernel holds its blocks until it ends: run it
+            # on a fraction of the SMs (blocks_per_sm of the usual 4-8), so
+            # that count batches launched meanwhile still find room
+            if enum_blocks_per_sm and hasattr(w, "set_tuning"):
+                w.set_tuning(block=128, blocks_per_sm=enum_blocks_per_sm, roots_per_fetch=32, steal_interval=16,
+                             min_split=2)
         self.enum_reqs: List[Optional[Request]] = [None] * enum_slots
         self.latencies: List[float] = []
+        # (kind, launch time, completion time, queries) of every launch
+        self.launch_log: List[tuple] = []
+        self.batch_t0: List[float] = [0.0] * inflight_batches
+        self.enum_t0: List[float] = [0.0] * enum_slots
         self.completed = 0
         self.limited = 0
         self.batches_launched = 0
@@ -122,7 +140,9 @@ class Server:
         return {"completed": self.completed, "limited": self.limited, "batches": self.batches_launched,
                 "queries_per_s": self.completed / span if span > 0 else 0.0,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
-                "p999_ms": float(np.percentile(lat, 99.9) * 1e3), "max_ms": float(lat.max() * 1e3)}
+                "p999_ms": float(np.percentile(lat, 99.9) * 1e3), "max_ms": float(lat.max() * 1e3),
+                "longest_launches_ms": sorted(([k, round((t1 - t0) * 1e3, 2), n] for k, t0, t1, n in self.launch_log),
+                                              key=lambda x: -x[1])[:5]}
 
     def drain(self, timeout_s: float = 600.0) -> None:
         t0 = time.time()
@@ -166,6 +186,7 @@ class Server:
         for i, b in enumerate(self.batches):
             reqs = self.batch_reqs[i]
             if reqs is not None and b.done():
+                self.launch_log.append(("batch", self.batch_t0[i], time.perf_counter(), len(reqs)))
                 counts = b.result()
                 b.clear()
                 self.batch_reqs[i] = None
@@ -176,6 +197,7 @@ class Server:
         for i, w in enumerate(self.enum_workers):
             r = self.enum_reqs[i]
             if r is not None and w.done():
+                self.launch_log.append(("enumerate", self.enum_t0[i], time.perf_counter(), 1))
                 try:
                     c, lim = w.result(), False
                 except capi.LimitExceeded:
@@ -209,6 +231,7 @@ class Server:
             for r in take:
                 b.add(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.flags)
             b.launch()
+            self.batch_t0[i] = time.perf_counter()
             self.batch_reqs[i] = take
             self.batches_launched += 1
             progressed = True
@@ -228,6 +251,7 @@ class Server:
                 self.enum_q.popleft()
             w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags)
             w.launch()
+            self.enum_t0[i] = time.perf_counter()
             self.enum_reqs[i] = r
             progressed = True
         return progressed
