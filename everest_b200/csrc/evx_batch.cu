@@ -1,13 +1,16 @@
-// Batched queries: many count queries against one resident graph in a single
-// persistent launch (include/everest_b200.h, evx_batch_*).
+// Batched queries: many count queries against one resident graph in one
+// persistent launch per motif size (include/everest_b200.h, evx_batch_*).
 //
-// The queries' root ranges are cut into tiles of tile_roots roots and laid
-// end to end as one device work queue; warps claim tiles with one atomicAdd
-// and switch their per-warp query copy when a tile belongs to another query,
-// so cheap and expensive queries share the GPU without per-query tails or
-// per-query launches.  The launch sequence (query table upload, counter
-// reset, kernel, counts read-back) is captured once into a CUDA graph and
-// replayed while the batch keeps the same shape.
+// The queries are ordered by motif size (stable); each size's queries form
+// one device work queue: their root ranges are cut into tiles of tile_roots
+// roots laid end to end, warps claim tiles with one atomicAdd and switch
+// their per-warp query copy when a tile belongs to another query, so cheap
+// and expensive queries share the GPU without per-query tails or per-query
+// launches.  Each size runs the kernel instantiated for exactly that size
+// (its levels are compile-time).  The launch sequence (query table upload,
+// counter reset, the kernels, counts read-back) is captured once into a CUDA
+// graph and replayed while the batch keeps the same shape.
+#include <algorithm>
 #include <climits>
 #include <cstdint>
 #include <cstring>
@@ -28,15 +31,20 @@ struct evx_batch {
   std::vector<QueryDesc> queries;
   QueryDesc *table_d = nullptr;        // [max_q]
   QueryDesc *table_h = nullptr;        // pinned [max_q]
-  unsigned long long *counts_d = nullptr;  // [max_q] counts, cursor word, [max_q] work meters
+  unsigned long long *counts_d = nullptr;  // [max_q] counts, kCursors cursor words, [max_q] work meters
   unsigned long long *counts_h = nullptr;  // pinned [max_q] counts, [max_q] meters
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // tuning
   int tile_roots = 256, blocks_per_sm = 0, steal_interval = 16, min_split = 2, use_graph = 1;
   unsigned long long limit = 0;  // work limit per query (0 = none)
+  // table order -> query index, and the motif-size groups of the table:
+  // {k, first table position, queries, tiles, grid}
+  std::vector<int> order;
+  std::vector<int> groups;
   // captured launch and the shape it was captured for
   cudaGraphExec_t exec = nullptr;
-  int exec_nq = -1, exec_kmax = -1, exec_tiles = -1, exec_grid = -1, exec_tile_roots = -1, exec_uniform = -1;
+  std::vector<int> exec_groups;
+  int exec_nq = -1, exec_tile_roots = -1;
   unsigned long long exec_limit = 0;
   const evx_graph *exec_graph = nullptr;
   bool launched = false;
@@ -46,35 +54,41 @@ struct evx_batch {
 
 namespace {
 
+constexpr int kCursors = 8;  // one work-queue cursor word per motif size
+
 void drop_exec(evx_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   b->exec = nullptr;
   b->exec_nq = -1;
 }
 
-int enqueue(evx_batch *b, int nq, int kmax, bool uniform, int total_tiles, int grid) {
-  int *cursor = reinterpret_cast<int *>(b->counts_d + b->max_q);
+int enqueue(evx_batch *b, int nq) {
+  unsigned long long *meter = b->counts_d + b->max_q + kCursors;
   EVX_CUDA(cudaMemcpyAsync(b->table_d, b->table_h, sizeof(QueryDesc) * (size_t)nq, cudaMemcpyHostToDevice,
                            b->stream));
-  EVX_CUDA(cudaMemsetAsync(b->counts_d, 0, sizeof(unsigned long long) * (2 * (size_t)b->max_q + 1), b->stream));
-  LaunchArgs la;
-  la.table = b->table_d;
-  la.nq = nq;
-  la.total_tiles = total_tiles;
-  la.tile_roots = b->tile_roots;
-  la.cursor = cursor;
-  la.counts = b->counts_d;
-  la.limit = b->limit;
-  la.meter = b->counts_d + b->max_q + 1;
-  if (total_tiles > 0) {
-    int rc = launch_table(b->graph->g.view(), b->table_h[0], la, kmax, uniform, grid, b->stream);
+  EVX_CUDA(cudaMemsetAsync(b->counts_d, 0, sizeof(unsigned long long) * (2 * (size_t)b->max_q + kCursors),
+                           b->stream));
+  for (size_t gi = 0; gi < b->groups.size(); gi += 5) {
+    const int k = b->groups[gi], beg = b->groups[gi + 1], n = b->groups[gi + 2];
+    const int tiles = b->groups[gi + 3], grid = b->groups[gi + 4];
+    if (tiles <= 0) continue;
+    LaunchArgs la;
+    la.table = b->table_d + beg;
+    la.nq = n;
+    la.total_tiles = tiles;
+    la.tile_roots = b->tile_roots;
+    la.cursor = reinterpret_cast<int *>(b->counts_d + b->max_q + gi / 5);
+    la.counts = b->counts_d + beg;
+    la.limit = b->limit;
+    la.meter = meter + beg;
+    int rc = launch_table(b->graph->g.view(), b->table_h[beg], la, k, grid, b->stream);
     if (rc) return rc;
     EVX_CUDA(cudaGetLastError());
   }
   EVX_CUDA(cudaMemcpyAsync(b->counts_h, b->counts_d, sizeof(unsigned long long) * (size_t)nq,
                            cudaMemcpyDeviceToHost, b->stream));
   if (b->limit)
-    EVX_CUDA(cudaMemcpyAsync(b->counts_h + b->max_q, la.meter, sizeof(unsigned long long) * (size_t)nq,
+    EVX_CUDA(cudaMemcpyAsync(b->counts_h + b->max_q, meter, sizeof(unsigned long long) * (size_t)nq,
                              cudaMemcpyDeviceToHost, b->stream));
   return EVX_OK;
 }
@@ -105,7 +119,7 @@ int evx_batch_create(int device, int max_queries, void *stream, evx_batch **out)
   }
   if (e == cudaSuccess) e = cudaMalloc(&b->table_d, sizeof(QueryDesc) * (size_t)max_queries);
   if (e == cudaSuccess) e = cudaMallocHost(&b->table_h, sizeof(QueryDesc) * (size_t)max_queries);
-  if (e == cudaSuccess) e = cudaMalloc(&b->counts_d, sizeof(unsigned long long) * (2 * (size_t)max_queries + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&b->counts_d, sizeof(unsigned long long) * (2 * (size_t)max_queries + kCursors));
   if (e == cudaSuccess) e = cudaMallocHost(&b->counts_h, sizeof(unsigned long long) * 2 * (size_t)max_queries);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&b->ev1);
@@ -206,38 +220,41 @@ int evx_batch_launch(evx_batch *b) {
   const int nq = (int)b->queries.size();
   if (nq == 0) return fail(EVX_ERR_STATE, "empty batch");
   EVX_CUDA(cudaSetDevice(b->device));
-  int kmax = 2, tiles = 0;
-  for (int i = 0; i < nq; i++) {
-    QueryDesc q = b->queries[i];
-    q.tile_beg = tiles;
-    const int n = q.root_end - q.root_beg;
-    tiles += n > 0 ? (n + b->tile_roots - 1) / b->tile_roots : 0;
-    if (q.plan.k > kmax) kmax = q.plan.k;
-    b->table_h[i] = q;
-  }
-  bool uniform = true;
-  for (int i = 0; i < nq; i++) uniform = uniform && b->table_h[i].plan.k == kmax;
-  int bps = b->blocks_per_sm;
-  if (bps <= 0) {
-    int rc = table_occupancy(kmax, uniform, &bps);  // also sets the kernel attributes before any capture
+  // table order: by motif size, stable; one group (and one launch) per size
+  b->order.resize(nq);
+  for (int i = 0; i < nq; i++) b->order[i] = i;
+  std::stable_sort(b->order.begin(), b->order.end(),
+                   [b](int x, int y) { return b->queries[x].plan.k < b->queries[y].plan.k; });
+  b->groups.clear();
+  int launches = 0;
+  for (int pos = 0; pos < nq;) {
+    const int k = b->queries[b->order[pos]].plan.k;
+    const int beg = pos;
+    int tiles = 0;
+    for (; pos < nq && b->queries[b->order[pos]].plan.k == k; pos++) {
+      QueryDesc q = b->queries[b->order[pos]];
+      q.tile_beg = tiles;
+      const int n = q.root_end - q.root_beg;
+      tiles += n > 0 ? (n + b->tile_roots - 1) / b->tile_roots : 0;
+      b->table_h[pos] = q;
+    }
+    int bps = 0;
+    int rc = table_occupancy(k, &bps);  // also sets the kernel attributes before any capture
     if (rc) return rc;
+    if (b->blocks_per_sm > 0) bps = b->blocks_per_sm;
     if (bps < 1) bps = 1;
-  } else {
-    int dummy = 0;
-    int rc = table_occupancy(kmax, uniform, &dummy);
-    if (rc) return rc;
+    b->groups.insert(b->groups.end(), {k, beg, pos - beg, tiles, bps * b->num_sms});
+    launches += tiles > 0 ? 1 : 0;
   }
-  const int grid = bps * b->num_sms;
+  if ((int)b->groups.size() / 5 > kCursors) return fail(EVX_ERR_INVALID, "too many motif sizes in one batch");
   EVX_CUDA(cudaEventRecord(b->ev0, b->stream));
   if (b->use_graph) {
-    if (!b->exec || b->exec_nq != nq || b->exec_kmax != kmax || b->exec_tiles != tiles ||
-        b->exec_uniform != (int)uniform ||
-        b->exec_grid != grid || b->exec_tile_roots != b->tile_roots || b->exec_graph != b->graph ||
-        b->exec_limit != b->limit) {
+    if (!b->exec || b->exec_nq != nq || b->exec_groups != b->groups || b->exec_tile_roots != b->tile_roots ||
+        b->exec_graph != b->graph || b->exec_limit != b->limit) {
       drop_exec(b);
       cudaGraph_t graph = nullptr;
       EVX_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-      int rc = enqueue(b, nq, kmax, uniform, tiles, grid);
+      int rc = enqueue(b, nq);
       cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
       if (rc) {
         if (graph) cudaGraphDestroy(graph);
@@ -247,17 +264,16 @@ int evx_batch_launch(evx_batch *b) {
       e = cudaGraphInstantiate(&b->exec, graph, 0);
       cudaGraphDestroy(graph);
       if (e != cudaSuccess) { b->exec = nullptr; return cuda_fail(e, "cudaGraphInstantiate"); }
-      b->exec_nq = nq; b->exec_kmax = kmax; b->exec_tiles = tiles; b->exec_grid = grid;
-      b->exec_uniform = (int)uniform;
+      b->exec_nq = nq; b->exec_groups = b->groups;
       b->exec_tile_roots = b->tile_roots; b->exec_graph = b->graph; b->exec_limit = b->limit;
     }
     EVX_CUDA(cudaGraphLaunch(b->exec, b->stream));
   } else {
-    int rc = enqueue(b, nq, kmax, uniform, tiles, grid);
+    int rc = enqueue(b, nq);
     if (rc) return rc;
   }
   EVX_CUDA(cudaEventRecord(b->ev1, b->stream));
-  b->last_launches = tiles > 0 ? 1 : 0;
+  b->last_launches = launches;
   b->launched = true;
   return EVX_OK;
 }
@@ -272,8 +288,11 @@ int evx_batch_result(evx_batch *b, uint64_t *counts, int n) {
   b->launched = false;
   const int nq = (int)b->queries.size();
   if (counts) {
-    for (int i = 0; i < n && i < nq; i++)
-      counts[i] = (b->limit && b->counts_h[b->max_q + i] > b->limit) ? UINT64_MAX : b->counts_h[i];
+    for (int pos = 0; pos < nq; pos++) {
+      const int i = b->order[pos];
+      if (i < n)
+        counts[i] = (b->limit && b->counts_h[b->max_q + pos] > b->limit) ? UINT64_MAX : b->counts_h[pos];
+    }
   }
   return EVX_OK;
 }

@@ -229,11 +229,10 @@ int cuda_fail(cudaError_t e, const char *what);
 int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &args,
                   int grid, int block, cudaStream_t stream);
 // Launch a persistent search over a table of queries (count mode); q0 is
-// used when nq == 1.  kmax = largest motif in the table; uniform = every
-// query has kmax edges (the exact-size kernel is used).
-int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int kmax, bool uniform,
-                 int grid, cudaStream_t stream);
-int table_occupancy(int kmax, bool uniform, int *blocks_per_sm);
+// used when nq == 1.  Every query of the table has k edges.
+int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int k, int grid,
+                 cudaStream_t stream);
+int table_occupancy(int k, int *blocks_per_sm);
 // Max resident blocks per SM for a given motif size / mode / block.
 int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm);
 

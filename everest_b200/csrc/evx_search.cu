@@ -993,19 +993,6 @@ constexpr int kSingleTileRoots = 64;
     case 8: return enumerate ? FN<8, true, true>(__VA_ARGS__) : FN<8, false, true>(__VA_ARGS__); \
     default: return fail(EVX_ERR_INVALID, "motif edge count out of range");          \
   }
-// query tables: count mode, motif sizes up to kmax
-#define EVX_T_DISPATCH(FN, ...)                                        \
-  switch (k) {                                                         \
-    case 2: return FN<2, false, false>(__VA_ARGS__);                   \
-    case 3: return FN<3, false, false>(__VA_ARGS__);                   \
-    case 4: return FN<4, false, false>(__VA_ARGS__);                   \
-    case 5: return FN<5, false, false>(__VA_ARGS__);                   \
-    case 6: return FN<6, false, false>(__VA_ARGS__);                   \
-    case 7: return FN<7, false, false>(__VA_ARGS__);                   \
-    case 8: return FN<8, false, false>(__VA_ARGS__);                   \
-    default: return fail(EVX_ERR_INVALID, "motif edge count out of range");          \
-  }
-
 int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &args, int grid, int block,
                   cudaStream_t stream) {
   (void)block;
@@ -1031,16 +1018,12 @@ int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &a
   EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
 }
 
-int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int kmax, bool uniform,
-                 int grid, cudaStream_t stream) {
-  const int k = kmax;
+int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int k, int grid,
+                 cudaStream_t stream) {
   const bool enumerate = false;
   EnumArgs ea;
   memset(&ea, 0, sizeof(ea));
-  // every query of size kmax: the exact-size kernel (its levels are
-  // compile-time, like a single query's)
-  if (uniform) EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
-  EVX_T_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
+  EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
 }
 
 int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm) {
@@ -1048,11 +1031,9 @@ int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm) {
   EVX_K_DISPATCH(occ_k, blocks_per_sm)
 }
 
-int table_occupancy(int kmax, bool uniform, int *blocks_per_sm) {
-  const int k = kmax;
+int table_occupancy(int k, int *blocks_per_sm) {
   const bool enumerate = false;
-  if (uniform) EVX_K_DISPATCH(occ_k, blocks_per_sm)
-  EVX_T_DISPATCH(occ_k, blocks_per_sm)
+  EVX_K_DISPATCH(occ_k, blocks_per_sm)
 }
 
 int search_block_size() { return kBlock; }

@@ -198,12 +198,13 @@ EVX_API int evx_worker_last_stats(evx_worker *w, int *kernel_launches, float *de
 EVX_API int evx_worker_set_limit(evx_worker *w, uint64_t max_work);
 
 /* -------------------------------------------------------------- batches --
- * Many count queries against one resident graph in a single persistent
- * launch (no counterpart in the reference, whose batch driver re-generates,
- * re-compiles and re-launches per query, system/batch-query.py:14-20 and
- * system/tmine/frontend.py:135-143).  Queries' root ranges are cut into
- * tiles that form one device work queue.  The launch sequence is captured
- * in a CUDA graph and replayed while the batch keeps its shape. */
+ * Many count queries against one resident graph in one persistent launch
+ * per motif size (no counterpart in the reference, whose batch driver
+ * re-generates, re-compiles and re-launches per query,
+ * system/batch-query.py:14-20 and system/tmine/frontend.py:135-143).  The
+ * root ranges of a size's queries are cut into tiles that form one device
+ * work queue.  The launch sequence is captured in a CUDA graph and replayed
+ * while the batch keeps its shape. */
 typedef struct evx_batch evx_batch;
 EVX_API int evx_batch_create(int device, int max_queries, void *stream, evx_batch **out);
 EVX_API int evx_batch_destroy(evx_batch *b);
