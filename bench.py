@@ -66,7 +66,7 @@ def parse():
                     help="batch/serve: roots per query (a random time window of the edge list)")
     ap.add_argument("--serve-slots", default="64,2,2,2",
                     help="serve: max queries per batch, batches in flight, enumeration slots, "
-                         "blocks per SM of an enumeration (0 = all)")
+                         "blocks per SM of an enumeration (0 = all)[, share of a batch kernel's blocks]")
     ap.add_argument("--limit", type=float, default=1e9,
                     help="batch/serve: work limit per query, in adjacency records examined inside "
                          "their time windows (stopped queries are flagged in both arms)")

@@ -160,13 +160,18 @@ def run_serve(args) -> int:
         fin[i] = prev
     seq_lat = fin - arr
     out = {}
-    slots = [int(x) for x in getattr(args, "serve_slots", "64,2,2,2").split(",")] + [2]
-    mb, ib, es, ebps = slots[:4]
-    runs = [("saturated", None)] * max(1, args.steps) + [("poisson", arr)]
+    slots = [float(x) for x in getattr(args, "serve_slots", "64,2,2,2").split(",")]
+    slots += [64, 2, 2, 2, 1.0][len(slots):]
+    mb, ib, es, ebps = (int(x) for x in slots[:4])
+    share = slots[4]
+    # untimed warm-up passes first (the device memory pool grows to its
+    # working size on the first pass), then the timed saturated passes
+    runs = ([("warmup", None)] * max(0, args.warmup) + [("saturated", None)] * max(1, args.steps)
+            + [("poisson", arr)])
     sat_runs = []
     for label, times in runs:
         srv = serve.Server(0, max_batch=mb, inflight_batches=ib, enum_slots=es, limit=limit,
-                           enum_blocks_per_sm=ebps)
+                           enum_blocks_per_sm=ebps, batch_share=share)
         for k, h in hosts.items():
             srv.add_graph(k, h)
         futs = []
@@ -186,7 +191,7 @@ def run_serve(args) -> int:
         st = srv.stats()
         if label == "saturated":
             sat_runs.append(st)
-        else:
+        elif label == "poisson":
             out[label] = st
         srv.close()
     # the saturated run is repeated (--steps times): the median run by
@@ -197,7 +202,7 @@ def run_serve(args) -> int:
     cnt = [i for i, q in enumerate(qs) if not q["cap"]]
     line = {"metric": "served queries/s and p50/p99/p99.9 latency vs one at a time, exact",
             "value": out["saturated"]["queries_per_s"], "unit": "queries/s", "n_gpus": 1, "steps": len(sat_runs),
-            "warmup": 1, "ms_per_step": 1e3 * n / max(out["saturated"]["queries_per_s"], 1e-9),
+            "warmup": max(0, args.warmup), "ms_per_step": 1e3 * n / max(out["saturated"]["queries_per_s"], 1e-9),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded generator)", "mode": "serve",
             "config": {"workload": f"bursty 7.8M + 63M edges resident; {n} queries, 3-5-edge patterns on 2-4 "
@@ -205,7 +210,7 @@ def run_serve(args) -> int:
                                    f"[1e4, 1e6]), roots = a random window of {window} edges per query",
                        "work_limit": limit, "poisson_rate_qps": rate,
                        "max_batch": mb, "batches_in_flight": ib, "enumeration_slots": es,
-                       "enumeration_blocks_per_sm": ebps},
+                       "enumeration_blocks_per_sm": ebps, "batch_share": share},
             "one_at_a_time": {"value": seq_qps, "unit": "queries/s",
                               "service_s": {"count": float(sum(svc[i] for i in cnt)),
                                             "enumerate": float(sum(svc[i] for i, q in enumerate(qs) if q["cap"])),

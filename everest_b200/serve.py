@@ -63,7 +63,7 @@ class Server:
     def __init__(self, device: int = 0, max_batch: int = 64, inflight_batches: int = 2,
                  enum_slots: int = 2, mem_reserve: int = 1 << 30, idle_sleep_s: float = 50e-6,
                  backend=None, limit: int = 0, use_graph: bool = False, tile_roots: int = 64,
-                 enum_blocks_per_sm: int = 2):
+                 enum_blocks_per_sm: int = 2, batch_share: float = 1.0):
         # backend: the module providing Batch, Worker, DeviceGraph and
         # device_mem_info (the C-ABI binding; tests substitute a fake)
         self.be = backend if backend is not None else capi
@@ -78,6 +78,12 @@ class Server:
         self.lock = threading.Lock()
         self.cv = threading.Condition(self.lock)
         self.limit = int(limit)
+        self.tile_roots = int(tile_roots)
+        self.use_graph = bool(use_graph)
+        # fraction of a batch kernel's usual resident blocks per SM: below 1,
+        # two batches in flight run side by side instead of the second one
+        # waiting for the first one's blocks
+        self.batch_share = float(batch_share)
         self.batches = [capi_.Batch(device, max_batch) for _ in range(inflight_batches)]
         for b in self.batches:
             if self.limit:
@@ -94,12 +100,11 @@ class Server:
         for w in self.enum_workers:
             if self.limit:
                 w.set_limit(self.limit)
-            # an enumeration's kernel holds its blocks until it ends: run it
-            # on a fraction of the SMs (blocks_per_sm of the usual 4-8), so
-            # that count batches launched meanwhile still find room
-            if enum_blocks_per_sm and hasattr(w, "set_tuning"):
-                w.set_tuning(block=128, blocks_per_sm=enum_blocks_per_sm, roots_per_fetch=32, steal_interval=16,
-                             min_split=2)
+        # an enumeration's kernel holds its blocks until it ends: while count
+        # work is queued or running, run it on a fraction of the SMs
+        # (blocks_per_sm of the usual 4-8) so that count batches still find
+        # room; with no count work about, on the whole GPU
+        self.enum_blocks_per_sm = int(enum_blocks_per_sm)
         self.enum_reqs: List[Optional[Request]] = [None] * enum_slots
         self.latencies: List[float] = []
         # (kind, launch time, completion time, queries) of every launch
@@ -230,6 +235,10 @@ class Server:
                 self.count_q = rest
             for r in take:
                 b.add(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.flags)
+            if self.batch_share < 1.0 and hasattr(b, "set_tuning"):
+                full = 8 if key[1] <= 3 else (6 if key[1] == 4 else 4)  # the kernels' register budgets
+                b.set_tuning(tile_roots=self.tile_roots, blocks_per_sm=max(1, int(full * self.batch_share)),
+                             use_graph=self.use_graph)
             b.launch()
             self.batch_t0[i] = time.perf_counter()
             self.batch_reqs[i] = take
@@ -250,6 +259,10 @@ class Server:
             with self.lock:
                 self.enum_q.popleft()
             w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags)
+            if self.enum_blocks_per_sm and hasattr(w, "set_tuning"):
+                busy = bool(self.count_q) or any(x is not None for x in self.batch_reqs)
+                w.set_tuning(block=128, blocks_per_sm=self.enum_blocks_per_sm if busy else 0, roots_per_fetch=32,
+                             steal_interval=16, min_split=2)
             w.launch()
             self.enum_t0[i] = time.perf_counter()
             self.enum_reqs[i] = r
