@@ -13,7 +13,7 @@ namespace evx {
 //   edges[e]    = {u, v, t, position of e in out_rec}     root fetch
 //   inpos[e]    = position of e in in_rec
 //   euid[e]     = original line id of e                    enumeration rows
-//   out_rec[p]  = {eid, v, t, position of eid in in_rec}   grouped by u, ascending eid
+//   out_rec[p]  = {eid, v, t, position of eid in in_rec (low 31 bits; see kPosMask)}   grouped by u, ascending eid
 //   in_rec[p]   = {eid, u, t, position of eid in out_rec}  grouped by v, ascending eid
 //   node_rng[x] = {out_beg, out_end, in_beg, in_end}       positions in out_rec / in_rec
 //   pair_rec[i] = {eid, t} grouped by static edge (u, v), ascending eid
@@ -57,6 +57,11 @@ __host__ __device__ inline unsigned long long pair_hash(unsigned long long x) {
   x ^= x >> 31;
   return x;
 }
+
+// The fourth word of an out_rec / in_rec record: the edge's position in its
+// other list in the low 31 bits; the top bit is set when the edge's pair run
+// (same endpoints, same direction) has a later entry.
+constexpr int kPosMask = 0x7fffffff;
 
 // Bit of a node in the 64-bit neighbour signatures (Fibonacci hashing; a
 // different hash from the pair table's).

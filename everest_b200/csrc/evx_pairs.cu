@@ -101,6 +101,17 @@ __global__ void cross_pos_kernel(const int4 *__restrict__ edges, const int4 *__r
   }
 }
 
+// Mark each adjacency record whose edge is followed by another entry of its
+// pair run (top bit of the record's fourth word).
+__global__ void mark_runs_kernel(int4 *__restrict__ out_rec, int4 *__restrict__ in_rec,
+                                 const int2 *__restrict__ loc, int n) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    const int2 lo = loc[out_rec[p].x], li = loc[in_rec[p].x];
+    if (lo.x + 1 < lo.y) out_rec[p].w |= (int)0x80000000u;
+    if (li.x + 1 < li.y) in_rec[p].w |= (int)0x80000000u;
+  }
+}
+
 // Neighbour signatures: one bit per neighbour (sig_bit) in each endpoint's word.
 __global__ void pair_sig_kernel(const int4 *__restrict__ edges, unsigned long long *__restrict__ sig_out,
                                 unsigned long long *__restrict__ sig_in, int n) {
@@ -276,6 +287,7 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     g.pair_max_probe = h[0];
     rev_loc_kernel<<<grid, block, 0, s>>>(g.view(), g.rev_loc, n);
     cross_pos_kernel<<<grid, block, 0, s>>>(g.edges, g.node_rng, g.out_rec, g.in_rec, g.cross_out, g.cross_in, n);
+    mark_runs_kernel<<<grid, block, 0, s>>>(g.out_rec, g.in_rec, g.pair_loc, n);
     EVX_CUDA(cudaGetLastError());
   }
 cleanup:

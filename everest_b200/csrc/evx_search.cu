@@ -351,7 +351,8 @@ struct Searcher {
     if (push) {
       const int s = nb + __popc(pm & lt);
       const int src = out ? base : rc.y, dst = out ? rc.y : base;
-      const int pop = out ? pos_found : rc.w, pip = out ? rc.w : pos_found;
+      const int pw = rc.w & kPosMask;
+      const int pop = out ? pos_found : pw, pip = out ? pw : pos_found;
       sm.task[l][s][0] = make_int4(parent, src, dst, rc.x);
       sm.task[l][s][1] = make_int4(rc.z, pop, pip, root);
     }
@@ -690,10 +691,14 @@ struct Searcher {
             // them): count the entries of that edge's own pair run (or of the
             // reverse pair's run) after the edge and inside the window
             const bool rev = (qf & kQRevPair) != 0;
+            // (a same-pair candidate whose record says its run ends with it
+            // adds nothing: skip its lookup)
             int2 pl[kScanWide];
 #pragma unroll
-            for (int q = 0; q < kScanWide; q++)
+            for (int q = 0; q < kScanWide; q++) {
+              if (!rev && rw[q].w >= 0) ok[q] = false;
               pl[q] = ok[q] ? __ldg((rev ? g.rev_loc : g.pair_loc) + rw[q].x) : make_int2(0, 0);
+            }
 #pragma unroll
             for (int q = 0; q < kScanWide; q++) {
               if (ok[q]) {
