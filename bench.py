@@ -250,6 +250,7 @@ def run_gpu_arm(args):
     qs = workloads.queries(args.workload)
     want = {r["name"]: r["count"] for r in stats["queries"]}
     bytes_alg = sum(r["bytes_alg"] for r in stats["queries"])
+    cands = sum(r["candidates"] for r in stats["queries"])  # edges visited by the serial semantics
 
     u, v, t = synth.load_or_generate(spec.name)
     host = capi.graph_build_host(u, v, t, name=spec.name)
@@ -365,6 +366,7 @@ def run_gpu_arm(args):
         "per_query_tuning": {k: "bps%d/steal%d/split%d/flags%d" % (c["blocks_per_sm"], c["steal_interval"],
                                                                      c["min_split"], c["flags"])
                              for k, c in tuned.items()},
+        "edges_visited_per_s": world * cands / (ms_per_step / 1e3),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} hbm_gbs",
