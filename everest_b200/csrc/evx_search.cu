@@ -163,6 +163,11 @@ __device__ __forceinline__ int pair_window(const GraphView &g, int start, int le
   return c - a;
 }
 
+// Count a task whose closing edge has few candidates from the closing side.
+#ifndef EVX_REVERSE_CLOSE
+#define EVX_REVERSE_CLOSE 1
+#endif
+
 // A new-node last edge's window is counted by range arithmetic when more than
 // this many records per already-mapped node remain (one pair probe each).
 #ifndef EVX_ARITH_RECS
@@ -630,7 +635,43 @@ struct Searcher {
           }
           hi = fa ? r.y : r.w;
         }
-        if (lo >= hi || ld_t(lst + lo) > tl) pos = end;
+        if (lo >= hi || ld_t(lst + lo) > tl) {
+          pos = end;
+        } else if (EVX_REVERSE_CLOSE && !ENUM && !strict_() && !(qf & (kQSamePair | kQRevPair))) {
+          // Few closing edges: count the task from the closing side.  Each
+          // closing edge e2 (x, c) inside the window pairs with the
+          // candidates e1 of this level that map the same new node c and
+          // come between the previous edge and e2, i.e. the entries of the
+          // pair (base, c) (or (c, base)) with edge id in (p, e2).  Taken
+          // when the window holds at most three closing edges and more
+          // candidates than that.
+          int4 c3[3];
+#pragma unroll
+          for (int j = 0; j < 3; j++) c3[j] = (lo + j < hi) ? __ldg(lst + lo + j) : make_int4(0, 0, INT_MAX, 0);
+          const bool more = lo + 3 < hi && ld_t(lst + lo + 3) <= tl;
+          int n2 = 0;
+#pragma unroll
+          for (int j = 0; j < 3; j++) n2 += c3[j].z <= tl ? 1 : 0;
+          const int4 *lst1 = out ? g.out_rec : g.in_rec;
+          if (!more && pos + n2 < end && ld_t(lst1 + pos + n2) <= tl) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+              if (j < n2) {
+                const int cn = c3[j].y;
+                bool fresh = true;
+#pragma unroll
+                for (int q = 0; q < N; q++) fresh = fresh && !(q < nmc && m[q] == cn);
+                const int a_ = out ? base : cn, b_ = out ? cn : base;
+                if (fresh && pair_maybe(g, a_, b_)) {
+                  const int2 f = pair_find(g, a_, b_);
+                  cnt += (unsigned long long)pair_count_eids(g, f.x, f.y, p.eid + 1, c3[j].x - 1);
+                }
+              }
+            }
+            cand += (unsigned)(n2 + 1);
+            pos = end;
+          }
+        }
       }
       while (true) {
         const unsigned act = __ballot_sync(kFull, pos < end);
