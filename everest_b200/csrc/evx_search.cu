@@ -167,6 +167,10 @@ __device__ __forceinline__ int pair_window(const GraphView &g, int start, int le
 #ifndef EVX_REVERSE_CLOSE
 #define EVX_REVERSE_CLOSE 1
 #endif
+#ifndef EVX_REV_MAX
+#define EVX_REV_MAX 8
+#endif
+constexpr int kRevMax = EVX_REV_MAX;  // most closing edges counted that way
 
 // A new-node last edge's window is counted by range arithmetic when more than
 // this many records per already-mapped node remain (one pair probe each).
@@ -643,19 +647,19 @@ struct Searcher {
           // candidates e1 of this level that map the same new node c and
           // come between the previous edge and e2, i.e. the entries of the
           // pair (base, c) (or (c, base)) with edge id in (p, e2).  Taken
-          // when the window holds at most three closing edges and more
+          // when the window holds at most kRevMax closing edges and more
           // candidates than that.
-          int4 c3[3];
+          int4 c3[kRevMax];
 #pragma unroll
-          for (int j = 0; j < 3; j++) c3[j] = (lo + j < hi) ? __ldg(lst + lo + j) : make_int4(0, 0, INT_MAX, 0);
-          const bool more = lo + 3 < hi && ld_t(lst + lo + 3) <= tl;
+          for (int j = 0; j < kRevMax; j++) c3[j] = (lo + j < hi) ? __ldg(lst + lo + j) : make_int4(0, 0, INT_MAX, 0);
+          const bool more = lo + kRevMax < hi && ld_t(lst + lo + kRevMax) <= tl;
           int n2 = 0;
 #pragma unroll
-          for (int j = 0; j < 3; j++) n2 += c3[j].z <= tl ? 1 : 0;
+          for (int j = 0; j < kRevMax; j++) n2 += c3[j].z <= tl ? 1 : 0;
           const int4 *lst1 = out ? g.out_rec : g.in_rec;
           if (!more && pos + n2 < end && ld_t(lst1 + pos + n2) <= tl) {
 #pragma unroll
-            for (int j = 0; j < 3; j++) {
+            for (int j = 0; j < kRevMax; j++) {
               if (j < n2) {
                 const int cn = c3[j].y;
                 bool fresh = true;
