@@ -136,6 +136,7 @@ __global__ void pair_insert_kernel(const unsigned long long *__restrict__ ukeys,
                                    unsigned long long mask, int *__restrict__ max_probe,
                                    int *__restrict__ overflow) {
   const int P = *num_runs;
+  int longest = 0;  // this thread's longest probe; one atomicMax per warp at the end
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
     const unsigned long long key = ukeys[p];
     unsigned long long h = pair_hash(key) & mask;
@@ -146,7 +147,7 @@ __global__ void pair_insert_kernel(const unsigned long long *__restrict__ ukeys,
       if (prev == ~0ull) {
         tab[h].z = starts[p];
         tab[h].w = lens[p];
-        atomicMax(max_probe, (int)i + 1);
+        longest = max(longest, (int)i + 1);
         done = true;
         break;
       }
@@ -154,6 +155,8 @@ __global__ void pair_insert_kernel(const unsigned long long *__restrict__ ukeys,
     }
     if (!done) atomicExch(overflow, 1);
   }
+  longest = __reduce_max_sync(0xffffffffu, (unsigned)longest);
+  if ((threadIdx.x & 31) == 0 && longest > 0) atomicMax(max_probe, longest);
 }
 
 }  // namespace
