@@ -211,7 +211,7 @@ struct GPUWorker {
   virtual std::vector<int> printEnum(int n);
   virtual std::pair<int, int> pause();
 
-  // Extensions of this build (query options the reference compiles into
+  // Extensions beyond the reference interface (query options it compiles into
   // each generated plugin): enumeration cap (0 = count), EVX_FLAG_* bits,
   // and the autotuner's launch parameters.
   virtual void configure(long long enumCap, unsigned flags);
