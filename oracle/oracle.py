@@ -29,6 +29,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_LIB_PATH = os.path.join(HERE, "_ref", "libref_baseline.so")
+REF_GPU_LIB_PATH = os.path.join(HERE, "_ref", "libref_baseline_gpu.so")
 
 _lib = None
 _ref = None
@@ -226,6 +227,46 @@ def ref_baseline_count(g: Graph, mu, mv, delta: int, roots=None, threads: int = 
     if rc != 0:
         raise ValueError("motif too large for the Baseline body (<=5 nodes, <=6 edges)")
     return int(out.value)
+
+
+_ref_gpu = None
+
+
+def ref_gpu_lib():
+    """The reference's Baseline kernel built for sm_100a, or None."""
+    global _ref_gpu
+    if _ref_gpu is None and os.path.exists(REF_GPU_LIB_PATH):
+        L = ctypes.CDLL(REF_GPU_LIB_PATH)
+        L.ref_gpu_count.argtypes = [_i32p, ctypes.c_int, _i32p, _i32p, _i32p, _i32p, ctypes.c_int,
+                                    _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong),
+                                    ctypes.POINTER(ctypes.c_float)]
+        L.ref_gpu_count.restype = ctypes.c_int
+        _ref_gpu = L
+    return _ref_gpu
+
+
+def ref_gpu_count(g: Graph, mu, mv, delta: int, reps: int = 2):
+    """(count, fastest ms of reps launches) of the reference's own Baseline
+    kernel on the GPU over every root (work = E - k + 1, as MineJob sets
+    it).  Raises RuntimeError when that build is absent."""
+    L = ref_gpu_lib()
+    if L is None:
+        raise RuntimeError("reference Baseline GPU build not present")
+    k = len(mu)
+    eg = np.stack([g.u, g.v, g.t], axis=1).astype(np.int32).ravel()
+    em = np.stack([np.asarray(mu, np.int32), np.asarray(mv, np.int32),
+                   np.arange(1, k + 1, dtype=np.int32)], axis=1).ravel()
+    out = ctypes.c_ulonglong(0)
+    ms = ctypes.c_float(0)
+    work = max(0, g.E - k + 1)
+    rc = L.ref_gpu_count(eg, g.E, g.in_eid, g.in_off, g.out_eid, g.out_off, g.V, em, k,
+                         motif_nodes(mu, mv), int(delta), work, int(reps), ctypes.byref(out), ctypes.byref(ms))
+    if rc == -1:
+        raise ValueError("motif too large for the Baseline kernel (<=5 nodes, <=6 edges)")
+    if rc != 0:
+        raise RuntimeError(f"reference Baseline kernel: CUDA error {rc}")
+    return int(out.value), float(ms.value)
 
 
 # ------------------------------------------------------------ brute force --

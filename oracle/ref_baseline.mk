@@ -18,3 +18,9 @@ $(OUT)/libref_baseline.so: $(SRC) $(HERE)ref_shim.h $(HERE)ref_driver.cc
 	tail -1 $(OUT)/baseline_body.inc | grep -q '^}'
 	g++ -O3 -march=x86-64-v2 -fopenmp -fPIC -shared -std=c++17 -I$(OUT) -I$(HERE) \
 	    -o $@ $(HERE)ref_driver.cc
+
+# Device build of the same kernel body for sm_100a (a parity and speed
+# comparator for the GPU tests; never linked by the product).
+$(OUT)/libref_baseline_gpu.so: $(OUT)/libref_baseline.so $(HERE)ref_gpu_driver.cu
+	nvcc -gencode arch=compute_100a,code=sm_100a -O3 -std=c++17 -Xcompiler -fPIC -shared \
+	    -I$(OUT) -o $@ $(HERE)ref_gpu_driver.cu
