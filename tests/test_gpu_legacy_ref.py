@@ -43,7 +43,7 @@ def test_reference_kernel_counts_equal_ours(ref):
         assert c == c_ref, (mu, mv, d, c, c_ref)
         t_ref += ms_ref
         t_ours += ms
-    print(f"\\n{len(qs)} queries on a 400k-edge bursty graph: reference Baseline kernel {t_ref:.2f} ms, "
+    print(f"\n{len(qs)} queries on a 400k-edge bursty graph: reference Baseline kernel {t_ref:.2f} ms, "
           f"this library {t_ours:.2f} ms ({t_ref / max(t_ours, 1e-9):.1f}x)")
     w.close()
     dg.free()
@@ -64,7 +64,7 @@ def test_reference_kernel_on_the_bench_graph(ref):
         assert c == c_ref, (q["name"], c, c_ref)
         t_ref += ms_ref
         t_ours += ms
-    print(f"\\n36 three-edge motifs on the 7.8M-edge graph: reference Baseline kernel {t_ref:.1f} ms, "
+    print(f"\n36 three-edge motifs on the 7.8M-edge graph: reference Baseline kernel {t_ref:.1f} ms, "
           f"this library (default launch parameters) {t_ours:.1f} ms ({t_ref / max(t_ours, 1e-9):.1f}x)")
     w.close()
     dg.free()
