@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--serve-slots", default="64,2,2,2",
                     help="serve: max queries per batch, batches in flight, enumeration slots, "
                          "blocks per SM of an enumeration (0 = all)[, share of a batch kernel's blocks]")
-    ap.add_argument("--limit", type=float, default=1e9,
+    ap.add_argument("--limit", type=float, default=1e8,
                     help="batch/serve: work limit per query, in adjacency records examined inside "
                          "their time windows (stopped queries are flagged in both arms)")
     return ap.parse_args()
