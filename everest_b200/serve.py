@@ -233,6 +233,9 @@ class Server:
                     (take if (r.graph, len(r.mu)) == key else rest).append(r)
                 rest.extend(self.count_q)
                 self.count_q = rest
+                # claimed under the lock: drain() never sees the requests in
+                # neither the queue nor a slot
+                self.batch_reqs[i] = take
             for r in take:
                 b.add(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.flags)
             if self.batch_share < 1.0 and hasattr(b, "set_tuning"):
@@ -241,7 +244,6 @@ class Server:
                              use_graph=self.use_graph)
             b.launch()
             self.batch_t0[i] = time.perf_counter()
-            self.batch_reqs[i] = take
             self.batches_launched += 1
             progressed = True
         # enumerate queries: admission by the memory their row buffers need
@@ -258,6 +260,7 @@ class Server:
                 break  # wait for running work to release memory
             with self.lock:
                 self.enum_q.popleft()
+                self.enum_reqs[i] = r  # claimed under the lock (see the batches above)
             w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags)
             if self.enum_blocks_per_sm and hasattr(w, "set_tuning"):
                 busy = bool(self.count_q) or any(x is not None for x in self.batch_reqs)
@@ -265,7 +268,6 @@ class Server:
                              steal_interval=16, min_split=2)
             w.launch()
             self.enum_t0[i] = time.perf_counter()
-            self.enum_reqs[i] = r
             progressed = True
         return progressed
 

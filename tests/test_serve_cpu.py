@@ -20,6 +20,8 @@ class FakeBackend:
         self.lock = threading.Lock()
         self.max_concurrent_enum = 0
         self.running_enum = 0
+        self.enum_bps = []  # blocks per SM asked for at each enumeration launch
+        self.batch_s = 0.002  # how long a launched batch takes
 
     def device_mem_info(self, device):
         with self.lock:
@@ -51,7 +53,7 @@ class FakeBackend:
                     c = O.count(gr, mu, mv, d, roots=(beg, max(beg, hi)))[0]
                     # the fake's work measure is the count itself
                     self.res.append(capi.LIMITED if self.limit and c > self.limit else c)
-                self.t_done = time.perf_counter() + 0.002
+                self.t_done = time.perf_counter() + be.batch_s
 
             def done(self):
                 return time.perf_counter() >= self.t_done
@@ -72,6 +74,9 @@ class FakeBackend:
         class W:
             def set_limit(self, n):
                 self.limit = n
+
+            def set_tuning(self, block, blocks_per_sm, roots_per_fetch, steal_interval, min_split):
+                be.enum_bps.append(blocks_per_sm)
 
             def take(self, g, mu, mv, d, beg, end, cap, flags):
                 self.args = (g, mu, mv, d, cap)
@@ -173,4 +178,22 @@ def test_root_ranges_and_count_limit(graph):
         else:
             assert not r.limited and r.count == c
     assert srv.stats()["limited"] == sum(c > limit for c in exact) == 1
+    srv.close()
+
+
+def test_enumerations_share_the_gpu_only_beside_count_work(graph):
+    # enumerations launched while count queries are queued or running take
+    # the configured fraction of the SMs; alone they take the whole GPU (0)
+    be = FakeBackend({"g": graph}, free_bytes=1 << 40)
+    be.batch_s = 0.2  # count batches still running when the first enumeration arrives
+    srv = serve.Server(max_batch=4, inflight_batches=1, enum_slots=1, mem_reserve=0, backend=be,
+                       enum_blocks_per_sm=2)
+    srv.add_graph("g", "g")
+    futs = [srv.submit("g", [0, 1, 2], [1, 2, 0], 2000) for _ in range(12)]
+    futs.append(srv.submit("g", [0, 1, 2], [1, 2, 0], 2000, enum_cap=10))
+    srv.drain(60)
+    futs.append(srv.submit("g", [0, 1, 2], [1, 2, 0], 2000, enum_cap=10))
+    srv.drain(60)
+    assert all(f.result(1) is not None for f in futs)
+    assert be.enum_bps[0] == 2 and be.enum_bps[-1] == 0
     srv.close()
