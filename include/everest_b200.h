@@ -249,6 +249,99 @@ EVX_API int evx_count_static(const evx_graph *g, int nq, const int *k, const int
                              const int *mv, const int *delta, int64_t beg, int64_t end,
                              unsigned flags, void *stream, uint64_t *counts);
 
+/* ---------------------------------------------------------- constraints --
+ * Replaces the reference's per-query generated constraint code
+ * (system/tmine/Query.py:39-310 renders C snippets that KernelGen.py:288-336,
+ * 467-533 and system/templates/common/{nextMatchInTask,structuralConstraint,
+ * lookAtMatchRes,findMatch}.snp compile into each plugin).  Here one
+ * precompiled kernel reads the constraints as data:
+ *
+ *   node predicates  (YAML `node: <expr in f>` or `node0..node{n-1}`): f is
+ *                    the node feature of the graph node a motif node maps to;
+ *   edge predicate   (YAML `edge: <expr in f>`): f is the edge feature of
+ *                    every matched edge (and of every anti-edge candidate);
+ *   temporal         (YAML `temporal: [g_0 .. g_{k-2}]`): motif edge j >= 1
+ *                    must have t <= t(previous real edge) + g_{j-1}, and for
+ *                    j >= 2 also t <= t(e_0) + delta (delta alone does not
+ *                    bound a two-edge motif with a temporal list, as in the
+ *                    reference: KernelGen.py:470-476);
+ *   anti-edges       (YAML `antiEdge: [bool x k]`): motif edge j must NOT
+ *                    exist: a partial match is dropped when some edge after
+ *                    the previous real edge, inside that edge's window, joins
+ *                    the two (already mapped) nodes and passes the edge
+ *                    predicate (lookAtMatchRes.snp:1-21);
+ *   filter           (YAML `filter: <expr in e0, e1, ...>`): e_i is the edge
+ *                    feature of the edge matched to motif edge i, evaluated
+ *                    once per complete match (findMatch.snp:1-8).
+ *
+ * Expressions are C integer expressions compiled to a postfix program: each
+ * instruction is op[i] | EVX_OP_WRAP32 (the result is an int: wrap it to 32
+ * bits) with arg[i] the constant or the variable index.  Values are int64;
+ * comparisons and logical operators give 0 or 1; division or remainder by
+ * zero gives 0; shifts use the count modulo the operand width. */
+#define EVX_PROG_MAX 48
+#define EVX_OP_CONST 1   /* push arg */
+#define EVX_OP_VAR 2     /* push variable arg (f = 0; e_i = i) */
+#define EVX_OP_NEG 3
+#define EVX_OP_NOT 4     /* logical ! */
+#define EVX_OP_BNOT 5    /* ~ */
+#define EVX_OP_ADD 6
+#define EVX_OP_SUB 7
+#define EVX_OP_MUL 8
+#define EVX_OP_DIV 9
+#define EVX_OP_MOD 10
+#define EVX_OP_SHL 11
+#define EVX_OP_SHR 12
+#define EVX_OP_LT 13
+#define EVX_OP_LE 14
+#define EVX_OP_GT 15
+#define EVX_OP_GE 16
+#define EVX_OP_EQ 17
+#define EVX_OP_NE 18
+#define EVX_OP_BAND 19
+#define EVX_OP_BXOR 20
+#define EVX_OP_BOR 21
+#define EVX_OP_LAND 22
+#define EVX_OP_LOR 23
+#define EVX_OP_COND 24   /* c ? a : b, pushed c, a, b */
+#define EVX_OP_WRAP32 0x80
+#define EVX_PROG_STACK 16
+
+typedef struct evx_program {
+  int32_t len;                 /* instructions (0 = always true) */
+  int32_t op[EVX_PROG_MAX];
+  int64_t arg[EVX_PROG_MAX];
+} evx_program;
+
+typedef struct evx_constraints {
+  uint32_t anti_mask;          /* bit j: motif edge j is an anti-edge */
+  int32_t has_temporal;
+  int32_t temporal[EVX_MAX_MOTIF_EDGES - 1];
+  int32_t node_mode;           /* 0 none, 1 node[0] for every node, 2 node[a] for motif node a */
+  evx_program node[EVX_MAX_MOTIF_NODES];
+  int32_t has_edge;
+  evx_program edge;
+  int32_t has_filter;
+  evx_program filter;
+} evx_constraints;
+
+/* Node features (int32 per graph vertex id) and edge features (int32 per
+ * sorted edge id) of a resident graph; either may be NULL (kept as before).
+ * Host arrays, copied to the graph's device. */
+EVX_API int evx_graph_set_features(evx_graph *g, const int *node_features, const int *edge_features);
+
+/* evx_worker_take with constraints (c may be NULL: plain search).  Checks
+ * what the reference cannot run: an anti-edge as motif edge 0, 1 or k-1
+ * (the generated search never ends or reads past its arrays there), an
+ * anti-edge touching a node that no earlier real edge maps, a filter naming
+ * an anti-edge, and enumeration with anti-edges (its rows would name no
+ * edge); node / edge predicates need the matching features on the graph.
+ * Flags: EVX_FLAG_EXACT_TOTAL only.  The plain search's launch, result and
+ * rows calls then run this job. */
+EVX_API int evx_worker_take_constrained(evx_worker *w, const evx_graph *g, int k, const int *mu,
+                                        const int *mv, int delta, int64_t beg, int64_t end,
+                                        int64_t enum_cap, unsigned flags, const evx_constraints *c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -303,3 +303,67 @@ def brute_force(u, v, t, mu, mv, delta: int, roots=None, strict_ts=False):
         if ok and len(set(phi.values())) == len(phi):
             out.append(combo)
     return out
+
+
+# ------------------------------------------------------------ constraints --
+def _cons_lib():
+    L = lib()
+    if not getattr(L, "_cons_ready", False):
+        args = [_i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_int, _i32p, _i32p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64]
+        L.oracle_count_constrained.argtypes = args + [ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]
+        L.oracle_count_constrained.restype = ctypes.c_int
+        L.oracle_enumerate_constrained.argtypes = args + [ctypes.c_void_p, ctypes.c_int64,
+                                                          ctypes.POINTER(ctypes.c_uint64)]
+        L.oracle_enumerate_constrained.restype = ctypes.c_int
+        L.oracle_prog_eval.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_prog_eval.restype = ctypes.c_int64
+        L._cons_ready = True
+    return L
+
+
+def _feat_ptr(a):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    return a, a.ctypes.data
+
+
+def count_constrained(g: Graph, mu, mv, delta: int, cons, node_feat=None, edge_feat=None,
+                      roots=None, threads: int = 0) -> int:
+    """Constrained count; cons is an everest_b200.constraints.EvxConstraints."""
+    k = len(mu)
+    rb, re_ = roots if roots is not None else default_roots(g, k)
+    a_mu, a_mv = _motif_arrays(mu, mv)
+    nf, ef = _feat_ptr(node_feat), _feat_ptr(edge_feat)
+    out = ctypes.c_uint64(0)
+    rc = _cons_lib().oracle_count_constrained(
+        *g._args(), nf[1] if nf else None, ef[1] if ef else None, k, a_mu, a_mv, int(delta),
+        ctypes.addressof(cons), int(rb), int(re_), int(threads), ctypes.byref(out))
+    if rc != 0:
+        raise ValueError("motif or constraints violate the search precondition")
+    return int(out.value)
+
+
+def enumerate_constrained(g: Graph, mu, mv, delta: int, cons, cap: int, node_feat=None,
+                          edge_feat=None, roots=None):
+    """Return (rows int32[min(cap,total), k] of sorted-edge ids, total)."""
+    k = len(mu)
+    rb, re_ = roots if roots is not None else default_roots(g, k)
+    a_mu, a_mv = _motif_arrays(mu, mv)
+    nf, ef = _feat_ptr(node_feat), _feat_ptr(edge_feat)
+    rows = np.zeros((max(cap, 1), k), np.int32)
+    tot = ctypes.c_uint64(0)
+    rc = _cons_lib().oracle_enumerate_constrained(
+        *g._args(), nf[1] if nf else None, ef[1] if ef else None, k, a_mu, a_mv, int(delta),
+        ctypes.addressof(cons), int(rb), int(re_), rows.ctypes.data, int(cap), ctypes.byref(tot))
+    if rc != 0:
+        raise ValueError("motif or constraints violate the search precondition")
+    n = min(cap, int(tot.value))
+    return rows[:n].copy(), int(tot.value)
+
+
+def prog_eval(prog, variables) -> int:
+    """The oracle's interpreter of one program (an EvxProgram)."""
+    vals = (ctypes.c_int64 * max(1, len(variables)))(*[int(x) for x in variables])
+    return int(_cons_lib().oracle_prog_eval(ctypes.addressof(prog), vals))

@@ -1,0 +1,174 @@
+"""Write constraint_golden.json: constrained counts computed by the
+reference's OWN generated search code, checked against the oracle.
+
+For every case the reference's KernelGen (system/tmine/KernelGen.py, run
+from a scratch copy of the reference's system/ tree, since it writes the
+constraint snippets into its template directory: Query.py:135-160) renders
+the per-query CUDA search with warpCentric, warpBalancing and tailExpansion
+off, so one CUDA thread runs one root's sequential search.  The kernel body
+(everything before the host launcher) is compiled for the host with
+gen_shim.h and run over every root by gen_driver.cc.  The oracle
+(oracle/evx_oracle_cons.c) must agree on every case, or nothing is written.
+
+Needs the reference tree (EVX_REFERENCE_ROOT, default /root/reference),
+g++ and PyYAML; run it where those exist:
+
+    python tests/golden/make_constraint_golden.py
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from everest_b200.constraints import Constraints  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+REF = os.environ.get("EVX_REFERENCE_ROOT", "/root/reference")
+GRAPHS = {"tiny-ties": 2, "dense-4": 20, "mid-ties": 5, "mid-uniform": 250, "mid-hub": 1000,
+          "zipf-2k-10k": 200000}
+MOTIFS = {
+    "path2": ([0, 1], [1, 2]),
+    "pair2": ([0, 1], [1, 0]),
+    "tri": ([0, 1, 2], [1, 2, 0]),
+    "star3": ([0, 0, 0], [1, 2, 3]),
+    "rep3": ([0, 1, 0], [1, 0, 1]),
+    "M4": ([0, 1, 2, 3], [1, 2, 3, 0]),
+    "M4-A": ([0, 1, 2, 2, 3], [1, 2, 0, 3, 0]),
+    "anti2": ([0, 1, 2, 1, 2, 3], [1, 2, 0, 0, 3, 0]),
+    "anti-fan": ([0, 1, 1, 0, 2], [1, 2, 0, 2, 0]),
+}
+ANTI = {"M4-A": [False, False, True, False, False],
+        "anti2": [False, False, True, True, False, False],
+        "anti-fan": [False, False, True, False, False]}
+PER_NODE = ["f % 2 == 0", "f < 7", "f != 3", "f >= 2", "(f & 1) || f > 5"]
+
+
+def constraint_sets(name, k, n, delta):
+    real = [j for j in range(k) if not ANTI.get(name, [False] * k)[j]]
+    gaps = [max(1, delta // (2 + (j % 3))) for j in range(k - 1)]
+    wide = [delta * 2] + [delta] * (k - 2)
+    filt = " + ".join(f"e{j}" for j in real if j < k - 1) + f" > {4 * max(1, len(real) - 1)}"
+    out = []
+    base = {"delta": delta}
+    if name in ANTI:
+        out.append(dict(base, antiEdge=ANTI[name]))
+        out.append(dict(base, antiEdge=ANTI[name], temporal=gaps))
+        out.append(dict(base, antiEdge=ANTI[name], node="f > 2", edge="f % 3 != 1"))
+        out.append(dict(base, antiEdge=ANTI[name], filter=filt,
+                        **{f"node{a}": PER_NODE[a % len(PER_NODE)] for a in range(n)}))
+        return out
+    out.append(dict(base, node="f > 4"))
+    out.append(dict(base, **{f"node{a}": PER_NODE[a % len(PER_NODE)] for a in range(n)}))
+    out.append(dict(base, edge="f % 3 != 1"))
+    out.append(dict(base, temporal=gaps))
+    out.append(dict(base, temporal=wide))
+    out.append(dict(base, filter=filt))
+    out.append(dict(base, node="-f < -1 && f * 3 <= 24", edge="(f ^ 5) > 2", temporal=gaps, filter=filt))
+    return out
+
+
+def load_kernelgen(scratch):
+    shutil.copytree(os.path.join(REF, "system"), os.path.join(scratch, "system"))
+    pkg = types.ModuleType("tmine")
+    pkg.__path__ = [os.path.join(scratch, "system", "tmine")]
+    sys.modules["tmine"] = pkg  # bypass tmine/__init__ (it imports the compiled corelib)
+    from tmine import KernelGen as KG, Query as Q  # noqa: E402
+    return KG, Q
+
+
+def render(KG, Q, scratch, mu, mv, cons):
+    motif = os.path.join(scratch, "motif.txt")
+    with open(motif, "w") as f:
+        for i, (a, b) in enumerate(zip(mu, mv)):
+            f.write(f"{a + 1} {b + 1} {i + 1}\n")
+    q = Q.Query.__new__(Q.Query)
+    q.queryFile = {"pattern": motif, "graph": "-", "constraints": cons,
+                   "options": {"gpu": 1, "warpCentric": False, "warpBalancing": False,
+                               "tailExpansion": False}}
+    q.name = "fixture"
+    q.cons = Q.Constraints(cons)
+    opts = Q.Options()
+    opts.update(Q.Options(q.queryFile["options"]))
+    q.opts = opts
+    q.cons.genConsTemplates()
+    src = KG.KernelGen(motif, q).generate()
+    body = []
+    for line in src.split("\n"):
+        if line.startswith("// -----"):
+            break
+        if line.lstrip().startswith("#include"):
+            continue
+        body.append(line)
+    return "\n".join(body) + "\n"
+
+
+def build_lib(scratch, body, tag):
+    inc = os.path.join(scratch, f"body_{tag}.inc")
+    with open(inc, "w") as f:
+        f.write(body)
+    so = os.path.join(scratch, f"gen_{tag}.so")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-w", "-fpermissive", f"-I{HERE}",
+                    f'-DGEN_BODY="{inc}"', "-o", so, os.path.join(HERE, "gen_driver.cc")], check=True)
+    L = ctypes.CDLL(so)
+    ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    L.gen_count.argtypes = [ip, ctypes.c_int, ip, ip, ip, ip, ip, ip, ip, ip, ctypes.c_int,
+                            ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong)]
+    L.gen_count.restype = ctypes.c_int
+    return L
+
+
+def main():
+    d = np.load(os.path.join(HERE, "small_graphs.npz"))
+    rng = np.random.Generator(np.random.PCG64(20261203))
+    feats = {}
+    cases = []
+    with tempfile.TemporaryDirectory() as scratch:
+        KG, Q = load_kernelgen(scratch)
+        tag = 0
+        for gname, delta in GRAPHS.items():
+            g = O.Graph(d[gname + "_u"], d[gname + "_v"], d[gname + "_t"], int(d[gname + "_V"][0]))
+            nf = rng.integers(0, 10, g.V).astype(np.int32)
+            ef = rng.integers(0, 10, max(g.E, 1)).astype(np.int32)
+            feats[gname + "_node"], feats[gname + "_edge"] = nf, ef
+            eg = np.stack([g.u, g.v, g.t], axis=1).astype(np.int32).ravel()
+            for mname, (mu, mv) in MOTIFS.items():
+                k, n = len(mu), max(max(mu), max(mv)) + 1
+                for cons in constraint_sets(mname, k, n, delta):
+                    body = render(KG, Q, scratch, mu, mv, cons)
+                    L = build_lib(scratch, body, tag)
+                    tag += 1
+                    work = max(0, g.E - k + 1)
+                    out = ctypes.c_ulonglong(0)
+                    L.gen_count(eg, g.E, g.in_eid, g.in_off, g.out_eid, g.out_off, nf, ef,
+                                np.asarray(mu, np.int32), np.asarray(mv, np.int32), k, delta, work,
+                                ctypes.byref(out))
+                    ref = int(out.value)
+                    c = Constraints.from_yaml(cons, mu, mv).to_struct()
+                    mine = O.count_constrained(g, mu, mv, delta, c, nf, ef)
+                    if mine != ref:
+                        raise SystemExit(f"oracle {mine} != reference {ref}: {gname} {mname} {cons}")
+                    cases.append({"graph": gname, "motif": mname, "mu": mu, "mv": mv, "delta": delta,
+                                  "constraints": cons, "count": ref})
+                    print(f"{gname:12s} {mname:8s} {ref:10d} {sorted(k for k in cons if k != 'delta')}")
+    np.savez_compressed(os.path.join(HERE, "constraint_features.npz"), **feats)
+    with open(os.path.join(HERE, "constraint_golden.json"), "w") as f:
+        json.dump({"source": "reference KernelGen output (warp options off) run on the host; "
+                             "oracle/evx_oracle_cons.c agrees on every case",
+                   "features": "constraint_features.npz", "cases": cases}, f, indent=0)
+    print(len(cases), "cases")
+
+
+if __name__ == "__main__":
+    main()
