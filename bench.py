@@ -56,11 +56,12 @@ def parse():
     ap.add_argument("--single-query", type=int, default=-1,
                     help="profiling aid: run only query I of the workload --reps times and exit")
     ap.add_argument("--reps", type=int, default=2)
-    ap.add_argument("--mode", default="single", choices=["single", "batch", "serve", "enumerate"],
+    ap.add_argument("--mode", default="single", choices=["single", "batch", "serve", "enumerate", "constrained"],
                     help="single: the 36-query per-query-kernel step (default); batch: 64 mixed queries "
                          "in one persistent launch per motif size vs the same queries one at a time; serve: "
                          "the serving loop (saturated and Poisson arrivals) vs one at a time; enumerate: "
-                         "the 36M-edge 4-cycle at cap 1e6 with a host check of the rows")
+                         "the 36M-edge 4-cycle at cap 1e6 with a host check of the rows; constrained: the "
+                         "reference's node / temporal / anti-edge / filter query shapes on the 7.8M graph")
     ap.add_argument("--queries", type=int, default=0, help="batch/serve: number of queries")
     ap.add_argument("--window", type=int, default=0,
                     help="batch/serve: roots per query (a random time window of the edge list)")
@@ -415,7 +416,7 @@ def main():
     args = parse()
     if args.single_query >= 0:
         return run_single_query(args)
-    if args.mode in ("batch", "serve", "enumerate"):
+    if args.mode in ("batch", "serve", "enumerate", "constrained"):
         from everest_b200 import bench_modes
         return bench_modes.run(args)
     if args.impl == "reference":

@@ -28,7 +28,8 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
 CXX_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-Wall", "-Wno-unused-function"]
 
-CORE_CU = ["evx_search.cu", "evx_graph.cu", "evx_pairs.cu", "evx_capi.cu", "evx_batch.cu", "evx_static.cu"]
+CORE_CU = ["evx_search.cu", "evx_graph.cu", "evx_pairs.cu", "evx_capi.cu", "evx_batch.cu", "evx_static.cu",
+           "evx_constrained.cu"]
 CORE_CC = ["evx_host.cc"]
 
 

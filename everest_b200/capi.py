@@ -44,7 +44,7 @@ EXPORTS = [
     "evx_batch_create", "evx_batch_destroy", "evx_batch_add", "evx_batch_clear", "evx_batch_launch",
     "evx_batch_result", "evx_batch_run", "evx_batch_set_tuning", "evx_batch_last_stats",
     "evx_device_mem_info", "evx_worker_query", "evx_batch_query", "evx_worker_set_limit",
-    "evx_batch_set_limit",
+    "evx_batch_set_limit", "evx_graph_set_features", "evx_worker_take_constrained",
 ]
 STATIC_MAX_QUERIES = 256
 
@@ -107,6 +107,9 @@ def lib():
             "evx_worker_destroy": ([_P], _I),
             "evx_worker_stream": ([_P, ctypes.POINTER(_P)], _I),
             "evx_worker_take": ([_P, _P, _I, _PI, _PI, _I, _I64, _I64, _I64, ctypes.c_uint], _I),
+            "evx_worker_take_constrained": ([_P, _P, _I, _PI, _PI, _I, _I64, _I64, _I64, ctypes.c_uint,
+                                             _P], _I),
+            "evx_graph_set_features": ([_P, _P, _P], _I),
             "evx_worker_run": ([_P, _PU64], _I),
             "evx_worker_launch": ([_P], _I),
             "evx_worker_result": ([_P, _PU64], _I),
@@ -196,6 +199,18 @@ class HostGraph:
         self.eg, self.out_v, self.in_v = eg, out_v, in_v
         self.out_r, self.in_r, self.euid = out_r, in_r, euid
         self.name = name
+
+    def original_vertex_ids(self, u, v, beg: int = 0) -> np.ndarray:
+        """Input vertex id of every relabeled vertex, given the input edge
+        arrays this graph was built from, starting at edge beg (node
+        features follow this map)."""
+        eg = self.eg.reshape(-1, 3)
+        src = np.asarray(u)[beg:beg + self.num_edges]
+        dst = np.asarray(v)[beg:beg + self.num_edges]
+        orig = np.full(self.num_vertices, -1, np.int64)
+        orig[eg[:, 0]] = src
+        orig[eg[:, 1]] = dst
+        return orig
 
     @property
     def total_bytes(self) -> int:
@@ -303,6 +318,17 @@ class DeviceGraph:
     def handle(self):
         return self._h
 
+    def set_features(self, node_features=None, edge_features=None) -> None:
+        """Node features (int32 per vertex id) and edge features (int32 per
+        sorted edge id) for constraint predicates and filters."""
+        nf = None if node_features is None else np.ascontiguousarray(node_features, dtype=np.int32)
+        ef = None if edge_features is None else np.ascontiguousarray(edge_features, dtype=np.int32)
+        if nf is not None and nf.size != self.num_vertices:
+            raise ValueError(f"{nf.size} node features for {self.num_vertices} vertices")
+        if ef is not None and ef.size != self.num_edges:
+            raise ValueError(f"{ef.size} edge features for {self.num_edges} edges")
+        check(lib().evx_graph_set_features(self._h, _ptr(nf), _ptr(ef)))
+
     def info(self):
         E, V, B = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         d = ctypes.c_int()
@@ -367,12 +393,20 @@ class Worker:
                                           steal_interval, min_split))
 
     def take(self, graph: DeviceGraph, mu: Sequence[int], mv: Sequence[int], delta: int,
-             beg: int = 0, end: int = -1, enum_cap: int = 0, flags: int = 0):
+             beg: int = 0, end: int = -1, enum_cap: int = 0, flags: int = 0, constraints=None):
+        """Bind a job; constraints (an everest_b200.constraints.Constraints or
+        its EvxConstraints struct) selects the constrained search."""
         k = len(mu)
         a_mu = (ctypes.c_int * k)(*mu)
         a_mv = (ctypes.c_int * k)(*mv)
-        check(lib().evx_worker_take(self._h, graph.handle, k, a_mu, a_mv, int(delta), int(beg),
-                                    int(end), int(enum_cap), int(flags)))
+        if constraints is None:
+            check(lib().evx_worker_take(self._h, graph.handle, k, a_mu, a_mv, int(delta), int(beg),
+                                        int(end), int(enum_cap), int(flags)))
+        else:
+            st = constraints.to_struct() if hasattr(constraints, "to_struct") else constraints
+            check(lib().evx_worker_take_constrained(self._h, graph.handle, k, a_mu, a_mv, int(delta),
+                                                    int(beg), int(end), int(enum_cap), int(flags),
+                                                    ctypes.byref(st)))
         self.k = k
         self.enum_cap = int(enum_cap)
 

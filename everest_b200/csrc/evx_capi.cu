@@ -154,6 +154,13 @@ struct evx_worker {
   int block = 256, blocks_per_sm = 0, roots_per_fetch = 32, steal_interval = 16, min_split = 2;
   int last_launches = 0;
   float last_ms = 0.f;
+  // constrained job (evx_worker_take_constrained)
+  bool cons_active = false;
+  ConsSearch cons{};
+  unsigned short *node_ok_d = nullptr;
+  int64_t node_ok_cap = 0;
+  unsigned char *edge_ok_d = nullptr;
+  int64_t edge_ok_cap = 0;
 };
 
 extern "C" {
@@ -322,6 +329,7 @@ int evx_graph_free(evx_graph *h) {
   dev_free(g.pair_loc, s); dev_free(g.pair_dir, s); dev_free(g.dir_off, s);
   dev_free(g.sig_out, s); dev_free(g.sig_in, s); dev_free(g.rev_loc, s);
   dev_free(g.cross_out, s); dev_free(g.cross_in, s);
+  dev_free(g.node_feat, s); dev_free(g.edge_feat, s);
   cudaStreamSynchronize(s);
   delete h;
   return EVX_OK;
@@ -372,6 +380,8 @@ int evx_worker_destroy(evx_worker *w) {
   if (!w) return EVX_OK;
   cudaSetDevice(w->device);
   if (w->rows_d && w->stream) dev_free(w->rows_d, w->stream);
+  if (w->node_ok_d && w->stream) dev_free(w->node_ok_d, w->stream);
+  if (w->edge_ok_d && w->stream) dev_free(w->edge_ok_d, w->stream);
   if (w->stream) cudaStreamSynchronize(w->stream);
   cudaFree(w->state_d);
   if (w->count_h) cudaFreeHost(w->count_h);
@@ -406,6 +416,31 @@ int evx_worker_set_tuning(evx_worker *w, int block, int blocks_per_sm, int roots
   return EVX_OK;
 }
 
+// Grow the worker's enumeration buffer to enum_cap rows of k ids, admitted
+// against free device memory.
+static int ensure_rows(evx_worker *w, int64_t enum_cap, int k) {
+  if (enum_cap <= 0) return EVX_OK;
+  if (enum_cap > (int64_t)INT_MAX) return fail(EVX_ERR_INVALID, "enumeration cap too large");
+  const int64_t need = enum_cap * (int64_t)k;
+  if (need > w->rows_cap) {
+    size_t fr = 0, tot = 0;
+    EVX_CUDA(cudaMemGetInfo(&fr, &tot));
+    const size_t bytes = (size_t)need * sizeof(int);
+    const size_t reserve = (size_t)256 << 20;  // keep headroom for other work
+    if (bytes + reserve > fr)
+      return fail(EVX_ERR_NOMEM, "enumeration buffer of " + std::to_string(bytes) +
+                                     " bytes not admitted (free " + std::to_string(fr) + ")");
+    // stream-ordered pool memory: no device-wide synchronisation, so a
+    // serving loop's other streams keep running while a buffer grows
+    int64_t grow = need;
+    if (2 * w->rows_cap > grow && (size_t)(2 * w->rows_cap) * sizeof(int) + reserve <= fr) grow = 2 * w->rows_cap;
+    if (w->rows_d) { dev_free(w->rows_d, w->stream); w->rows_d = nullptr; w->rows_cap = 0; }
+    EVX_CUDA(dev_alloc((void **)&w->rows_d, (size_t)grow * sizeof(int), w->device, w->stream));
+    w->rows_cap = grow;
+  }
+  return EVX_OK;
+}
+
 int evx_worker_take(evx_worker *w, const evx_graph *gh, int k, const int *mu, const int *mv,
                     int delta, int64_t beg, int64_t end, int64_t enum_cap, unsigned flags) {
   if (!w || !gh || !mu || !mv) return fail(EVX_ERR_INVALID, "null argument");
@@ -424,26 +459,8 @@ int evx_worker_take(evx_worker *w, const evx_graph *gh, int k, const int *mu, co
   if (beg < 0) beg = 0;
   if (end < beg) end = beg;
   EVX_CUDA(cudaSetDevice(w->device));
-  if (enum_cap > 0) {
-    if (enum_cap > (int64_t)INT_MAX) return fail(EVX_ERR_INVALID, "enumeration cap too large");
-    const int64_t need = enum_cap * (int64_t)k;
-    if (need > w->rows_cap) {
-      size_t fr = 0, tot = 0;
-      EVX_CUDA(cudaMemGetInfo(&fr, &tot));
-      const size_t bytes = (size_t)need * sizeof(int);
-      const size_t reserve = (size_t)256 << 20;  // keep headroom for other work
-      if (bytes + reserve > fr)
-        return fail(EVX_ERR_NOMEM, "enumeration buffer of " + std::to_string(bytes) +
-                                       " bytes not admitted (free " + std::to_string(fr) + ")");
-      // stream-ordered pool memory: no device-wide synchronisation, so a
-      // serving loop's other streams keep running while a buffer grows
-      int64_t grow = need;
-      if (2 * w->rows_cap > grow && (size_t)(2 * w->rows_cap) * sizeof(int) + reserve <= fr) grow = 2 * w->rows_cap;
-      if (w->rows_d) { dev_free(w->rows_d, w->stream); w->rows_d = nullptr; w->rows_cap = 0; }
-      EVX_CUDA(dev_alloc((void **)&w->rows_d, (size_t)grow * sizeof(int), w->device, w->stream));
-      w->rows_cap = grow;
-    }
-  }
+  rc = ensure_rows(w, enum_cap, k);
+  if (rc) return rc;
   w->view = g.view();
   w->plan = plan;
   SearchArgs &a = w->args;
@@ -466,6 +483,137 @@ int evx_worker_take(evx_worker *w, const evx_graph *gh, int k, const int *mu, co
   a.limit = (unsigned long long)w->limit;
   a.meter = w->state_d + 2;
   w->enum_cap = enum_cap;
+  w->cons_active = false;
+  w->has_job = true;
+  w->launched = false;
+  return EVX_OK;
+}
+
+int evx_graph_set_features(evx_graph *h, const int *node_features, const int *edge_features) {
+  if (!h) return fail(EVX_ERR_INVALID, "null graph");
+  DeviceGraph &g = h->g;
+  EVX_CUDA(cudaSetDevice(g.device));
+  auto put = [&](int **dst, const int *src, int64_t n) -> int {
+    if (!src) return EVX_OK;
+    if (!*dst) {
+      EVX_CUDA(dev_alloc((void **)dst, sizeof(int) * (size_t)(n > 0 ? n : 1), g.device, nullptr));
+      g.bytes += sizeof(int) * (n > 0 ? n : 1);
+    }
+    if (n > 0) EVX_CUDA(cudaMemcpyAsync(*dst, src, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, nullptr));
+    return EVX_OK;
+  };
+  int rc = put(&g.node_feat, node_features, g.num_vertices);
+  if (!rc) rc = put(&g.edge_feat, edge_features, g.num_edges);
+  EVX_CUDA(cudaStreamSynchronize(nullptr));
+  return rc;
+}
+
+int evx_worker_take_constrained(evx_worker *w, const evx_graph *gh, int k, const int *mu, const int *mv,
+                                int delta, int64_t beg, int64_t end, int64_t enum_cap, unsigned flags,
+                                const evx_constraints *c) {
+  if (!c) return evx_worker_take(w, gh, k, mu, mv, delta, beg, end, enum_cap, flags);
+  if (!w || !gh || !mu || !mv) return fail(EVX_ERR_INVALID, "null argument");
+  if (gh->g.device != w->device) return fail(EVX_ERR_INVALID, "graph and worker on different devices");
+  if (flags & ~EVX_FLAG_EXACT_TOTAL)
+    return fail(EVX_ERR_INVALID, "constrained searches take no flag but EVX_FLAG_EXACT_TOTAL");
+  MotifPlan plan;
+  int rc = build_plan(k, mu, mv, &plan);
+  if (rc) return rc;
+  const DeviceGraph &g = gh->g;
+  if (delta < 0) return fail(EVX_ERR_INVALID, "delta must be non-negative");
+  if ((int64_t)g.max_t + (int64_t)delta > (int64_t)INT_MAX)
+    return fail(EVX_ERR_OVERFLOW, "t + delta overflows int32");
+  // anti-edges: never motif edge 0, 1 or k-1; both ends mapped by earlier real edges
+  if (c->anti_mask >> k) return fail(EVX_ERR_INVALID, "anti-edge mask names edges past the motif");
+  if (c->anti_mask & (1u | 2u | (1u << (k - 1))))
+    return fail(EVX_ERR_INVALID, "motif edges 0, 1 and k-1 cannot be anti-edges");
+  unsigned mapped = (1u << mu[0]) | (1u << mv[0]);
+  ConsSearch cs;
+  std::memset(&cs, 0, sizeof(cs));
+  for (int j = 1; j < k; j++) {
+    const bool anti = (c->anti_mask >> j) & 1;
+    if (anti && !(((mapped >> mu[j]) & 1) && ((mapped >> mv[j]) & 1)))
+      return fail(EVX_ERR_INVALID, "anti-edge " + std::to_string(j) + " touches a node no earlier real edge maps");
+    if (!anti) mapped |= (1u << mu[j]) | (1u << mv[j]);
+    int p = j - 1;
+    while (p > 0 && ((c->anti_mask >> p) & 1)) p--;
+    cs.prev_real[j] = p;
+  }
+  if (c->anti_mask && enum_cap > 0)
+    return fail(EVX_ERR_INVALID, "enumeration with anti-edges is not supported (rows would name no edge)");
+  if (c->has_temporal) {
+    for (int j = 0; j < k - 1; j++) {
+      const int64_t gap = c->temporal[j];
+      if ((int64_t)g.max_t + gap > (int64_t)INT_MAX || (int64_t)g.min_t + gap < (int64_t)INT_MIN)
+        return fail(EVX_ERR_OVERFLOW, "t + temporal gap overflows int32");
+      cs.temporal[j] = (int)gap;
+    }
+  }
+  if (c->node_mode < 0 || c->node_mode > 2) return fail(EVX_ERR_INVALID, "bad node_mode");
+  if (c->node_mode) {
+    if (!g.node_feat) return fail(EVX_ERR_STATE, "node predicates need node features on the graph");
+    for (int a = 0; a < (c->node_mode == 1 ? 1 : plan.n); a++) {
+      rc = cons_check_program(c->node[a], 1, "node predicate");
+      if (rc) return rc;
+    }
+  }
+  if (c->has_edge) {
+    if (!g.edge_feat) return fail(EVX_ERR_STATE, "an edge predicate needs edge features on the graph");
+    rc = cons_check_program(c->edge, 1, "edge predicate");
+    if (rc) return rc;
+  }
+  if (c->has_filter) {
+    if (!g.edge_feat) return fail(EVX_ERR_STATE, "a filter needs edge features on the graph");
+    rc = cons_check_program(c->filter, k, "filter");
+    if (rc) return rc;
+    for (int i = 0; i < c->filter.len; i++)
+      if ((c->filter.op[i] & 0x7f) == EVX_OP_VAR && ((c->anti_mask >> c->filter.arg[i]) & 1))
+        return fail(EVX_ERR_INVALID, "the filter names an anti-edge");
+  }
+  const int64_t E = g.num_edges, V = g.num_vertices;
+  if (end < 0) end = E - k + 1;
+  if (end > E) end = E;
+  if (beg < 0) beg = 0;
+  if (end < beg) end = beg;
+  EVX_CUDA(cudaSetDevice(w->device));
+  rc = ensure_rows(w, enum_cap, k);
+  if (rc) return rc;
+  if (c->node_mode && V > w->node_ok_cap) {
+    if (w->node_ok_d) { dev_free(w->node_ok_d, w->stream); w->node_ok_d = nullptr; w->node_ok_cap = 0; }
+    EVX_CUDA(dev_alloc((void **)&w->node_ok_d, sizeof(unsigned short) * (size_t)V, w->device, w->stream));
+    w->node_ok_cap = V;
+  }
+  if (c->has_edge && E > w->edge_ok_cap) {
+    if (w->edge_ok_d) { dev_free(w->edge_ok_d, w->stream); w->edge_ok_d = nullptr; w->edge_ok_cap = 0; }
+    EVX_CUDA(dev_alloc((void **)&w->edge_ok_d, (size_t)E, w->device, w->stream));
+    w->edge_ok_cap = E;
+  }
+  rc = cons_build_masks(*c, plan.n, g.node_feat, (int)V, g.edge_feat, (int)E, w->node_ok_d, w->edge_ok_d,
+                        w->num_sms, w->stream);
+  if (rc) return rc;
+  cs.plan = plan;
+  cs.root_beg = (int)beg;
+  cs.root_end = (int)end;
+  cs.delta = delta;
+  cs.anti_mask = c->anti_mask;
+  cs.has_temporal = c->has_temporal ? 1 : 0;
+  cs.has_filter = c->has_filter ? 1 : 0;
+  cs.exact_total = (flags & EVX_FLAG_EXACT_TOTAL) ? 1 : 0;
+  cs.filter = c->filter;
+  cs.node_ok = c->node_mode ? w->node_ok_d : nullptr;
+  cs.edge_ok = c->has_edge ? w->edge_ok_d : nullptr;
+  cs.edge_feat = g.edge_feat;
+  cs.count = w->state_d;
+  cs.cursor = reinterpret_cast<int *>(w->state_d + 1);
+  cs.stop = reinterpret_cast<int *>(w->state_d + 1) + 1;
+  cs.rows = w->rows_d;
+  cs.cap = enum_cap;
+  w->view = g.view();
+  w->plan = plan;
+  std::memset(&w->args, 0, sizeof(w->args));  // no work limit on constrained jobs
+  w->cons = cs;
+  w->cons_active = true;
+  w->enum_cap = enum_cap;
   w->has_job = true;
   w->launched = false;
   return EVX_OK;
@@ -479,6 +627,36 @@ __global__ void reset_state_kernel(unsigned long long *count, int *cursor, int *
   count[2] = 0ull;  // work meter
 }
 }  // namespace evx
+
+// Launch of a job taken by evx_worker_take_constrained: state reset, then
+// one constrained search over the job's roots.
+static int launch_constrained_job(evx_worker *w) {
+  ConsSearch &c = w->cons;
+  int bps = w->blocks_per_sm;
+  if (bps <= 0) {
+    int rc = cons_occupancy(c.plan.k, w->enum_cap > 0, &bps);
+    if (rc) return rc;
+    if (bps <= 0) bps = 1;
+  }
+  const int grid = bps * w->num_sms;
+  if ((int64_t)c.root_end + (int64_t)grid * cons_block() >= (int64_t)INT_MAX)
+    return fail(EVX_ERR_OVERFLOW, "root cursor would overflow int32");
+  reset_state_kernel<<<1, 1, 0, w->stream>>>(c.count, c.cursor, c.stop, c.root_beg);
+  EVX_CUDA(cudaGetLastError());
+  EVX_CUDA(cudaEventRecord(w->ev0, w->stream));
+  int launches = 1;
+  if (c.root_end > c.root_beg) {
+    int rc = launch_constrained(w->view, c, w->enum_cap > 0, grid, w->stream);
+    if (rc) return rc;
+    launches++;
+  }
+  EVX_CUDA(cudaEventRecord(w->ev1, w->stream));
+  EVX_CUDA(cudaMemcpyAsync(w->count_h, c.count, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           w->stream));
+  w->last_launches = launches;
+  w->launched = true;
+  return EVX_OK;
+}
 
 int evx_worker_launch(evx_worker *w) {
   if (!w) return fail(EVX_ERR_INVALID, "null worker");
@@ -495,6 +673,7 @@ int evx_worker_launch(evx_worker *w) {
   const int64_t warps = (int64_t)grid * (w->block / 32);
   if ((int64_t)a.root_end + warps * (int64_t)a.roots_per_fetch >= (int64_t)INT_MAX)
     return fail(EVX_ERR_OVERFLOW, "root cursor would overflow int32");
+  if (w->cons_active) return launch_constrained_job(w);
   reset_state_kernel<<<1, 1, 0, w->stream>>>(a.count, a.cursor, a.stop, 0);
   EVX_CUDA(cudaGetLastError());
   EVX_CUDA(cudaEventRecord(w->ev0, w->stream));

@@ -192,6 +192,7 @@ struct DeviceGraph {
   int2 *pair_dir = nullptr;
   int *dir_off = nullptr;
   unsigned long long *sig_out = nullptr, *sig_in = nullptr;
+  int *node_feat = nullptr, *edge_feat = nullptr;  // constraint features (optional)
   unsigned long long pair_mask = 0;
   int pair_max_probe = 0;
   int64_t bytes = 0;
@@ -240,6 +241,37 @@ int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, 
 int table_occupancy(int k, int *blocks_per_sm);
 // Max resident blocks per SM for a given motif size / mode / block.
 int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm);
+
+// A constrained search (evx_constrained.cu).  prev_real[j] = the latest motif
+// edge before j that is not an anti-edge (0 for j = 1).
+struct ConsSearch {
+  MotifPlan plan;
+  int root_beg, root_end;
+  int delta;
+  unsigned anti_mask;                        // bit j: motif edge j is an anti-edge
+  int prev_real[EVX_MAX_MOTIF_EDGES];
+  int has_temporal;
+  int temporal[EVX_MAX_MOTIF_EDGES];         // [j-1]: gap bound of motif edge j
+  int has_filter;
+  int exact_total;                           // enumerate: keep counting past the cap
+  evx_program filter;                        // variables e_0 .. e_{k-1}
+  const unsigned short *node_ok;             // [V] bit a: may be motif node a (null: all)
+  const unsigned char *edge_ok;              // [E] edge predicate (null: all)
+  const int *edge_feat;                      // [E] filter variables
+  unsigned long long *count;                 // result / enumeration slot counter
+  int *cursor;                               // next unclaimed root id
+  int *stop;                                 // set when the enumeration cap is reached
+  int *rows;                                 // [cap * k] original line ids
+  long long cap;
+};
+int launch_constrained(const GraphView &g, const ConsSearch &s, bool enumerate, int grid, cudaStream_t st);
+int cons_occupancy(int k, bool enumerate, int *blocks_per_sm);
+int cons_block();
+// Host check of a program's opcodes, stack use and variable indices.
+int cons_check_program(const evx_program &p, int num_vars, const char *what);
+// Node bit sets and edge flags from the predicates (no-ops for absent ones).
+int cons_build_masks(const evx_constraints &c, int n, const int *node_feat, int V, const int *edge_feat,
+                     int E, unsigned short *node_ok, unsigned char *edge_ok, int num_sms, cudaStream_t s);
 
 // Build the pair index (defined in evx_pairs.cu); needs edges[] packed.
 int build_pair_index(DeviceGraph &g, cudaStream_t s);
