@@ -352,7 +352,7 @@ def run_constrained(args) -> int:
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator and features)",
             "mode": "constrained",
             "config": {"workload": "bursty 1.1M nodes / 7.8M edges, node and edge features U[0, 1e9); "
-                                   "4-cycle and 4-cycle with anti-edge, delta 3600"},
+                                   "4-cycle and 4-cycle with anti-edge, delta 86400, gaps 21600 / 43200"},
             "queries": out, "plain_kernel_M4_count": int(plain),
             "cpu_baseline": {"value": len(out) / sum(q["oracle_ms_all_cores"] / 1e3 for q in out),
                              "unit": "queries/s", "cores": os.cpu_count(), "kind": "port",

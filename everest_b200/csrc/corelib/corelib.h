@@ -10,8 +10,10 @@
 //    std::invalid_argument (ValueError); nothing calls exit();
 //  * one prebuilt plugin serves every motif: the motif is bound at take()
 //    time from DeviceJobData, so no per-query code generation or nvcc;
-//  * FeatureLoader accepts a missing random-feature file (labels are not on
-//    this path);
+//  * FeatureLoader accepts a missing random-feature file (only queries with
+//    node / edge predicates or a filter need it);
+//  * query constraints reach the worker as data (GPUWorker::setConstraints),
+//    not as generated code;
 //  * multi-GPU execution classes exist but refuse more than one device.
 #pragma once
 
@@ -74,17 +76,23 @@ class EdgeListLoader : public CacheDirectoryAccess {
   std::vector<int> U_, V_, T_, IDS_;
 };
 
-// Random per-edge / per-vertex features (src/core/cpu/data.cc:316-343).
-// Labels are not used by this path; a missing file yields empty features.
+// Random per-edge / per-vertex features (src/core/cpu/data.cc:316-343,
+// src/core/gpu/data.cu:57-79): a raw int32 file whose first E values are the
+// features of the time-sorted edges and whose first N values those of the N
+// distinct vertex ids in ascending order.  A missing or short file yields
+// empty features (queries without node / edge predicates need none).
 class FeatureLoader : public CacheDirectoryAccess {
  public:
   FeatureLoader(const EdgeListLoader *eloader, const std::filesystem::path &pathToRands);
   size_t edgeFeaturesLength() const { return edge_.size(); }
   size_t verticesFeaturesLength() const { return vertex_.size(); }
   const std::vector<int> &edgeFeatures() const { return edge_; }
+  // feature of an input vertex id (0 when the file held no vertex features)
+  int vertexFeature(int id) const;
+  bool hasVertexFeatures() const { return !vertex_.empty(); }
 
  private:
-  std::vector<int> edge_, vertex_;
+  std::vector<int> edge_, vertex_, vertexIds_;
 };
 
 // The graph data for a subset [beg, end) of the edge list
@@ -219,6 +227,10 @@ struct GPUWorker {
                          int minSplit);
   virtual double lastDeviceMs() const;
   virtual int lastKernelLaunches() const;
+  // Query constraints (node / edge predicates, temporal gaps, anti-edges,
+  // filters), which the reference compiles into each generated plugin;
+  // nullptr clears them.  Applies from the next take().
+  virtual void setConstraints(const evx_constraints *c);
 };
 
 // The B200 worker behind the plugin.
@@ -234,9 +246,12 @@ struct GPUWorkerEVX : public GPUWorker {
                  int minSplit) override;
   double lastDeviceMs() const override;
   int lastKernelLaunches() const override;
+  void setConstraints(const evx_constraints *c) override;
 
  private:
   evx_worker *w_ = nullptr;
+  bool hasCons_ = false;
+  evx_constraints cons_{};
   long long enumCap_ = 0;
   unsigned flags_ = 0;
   int k_ = 0;

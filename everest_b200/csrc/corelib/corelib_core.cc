@@ -97,9 +97,24 @@ EdgeListLoader::EdgeListLoader(const std::filesystem::path &pathToGraph, bool us
 FeatureLoader::FeatureLoader(const EdgeListLoader *eloader, const std::filesystem::path &pathToRands)
     : CacheDirectoryAccess(eloader->graphPath_, false) {
   std::vector<int> r;
-  if (!pathToRands.empty() && read_ints(pathToRands, r) && r.size() >= eloader->edgeListLength()) {
-    edge_.assign(r.begin(), r.begin() + (long)eloader->edgeListLength());
+  if (pathToRands.empty() || !read_ints(pathToRands, r)) return;
+  const size_t E = eloader->edgeListLength();
+  if (r.size() >= E) edge_.assign(r.begin(), r.begin() + (long)E);
+  // distinct vertex ids, ascending; vertex i of that order takes value i
+  std::vector<int> ids(eloader->U());
+  ids.insert(ids.end(), eloader->V().begin(), eloader->V().end());
+  std::sort(ids.begin(), ids.end());
+  ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+  if (r.size() >= ids.size()) {
+    vertex_.assign(r.begin(), r.begin() + (long)ids.size());
+    vertexIds_ = std::move(ids);
   }
+}
+
+int FeatureLoader::vertexFeature(int id) const {
+  auto it = std::lower_bound(vertexIds_.begin(), vertexIds_.end(), id);
+  if (it == vertexIds_.end()) return 0;
+  return vertex_[(size_t)(it - vertexIds_.begin())];
 }
 
 SubPartitionList divideList(const EdgeListLoader &eloader, int delta, int num) {
@@ -187,6 +202,15 @@ HostGraphData GraphDataLoader::createGraphData(size_t beg, size_t end, bool cach
   res.Euid = take_ints(eu, (size_t)E);
   const auto &fe = floader_ ? floader_->edgeFeatures() : std::vector<int>();
   if (fe.size() >= end) res.edgeFeatures.assign(fe.begin() + (long)beg, fe.begin() + (long)end);
+  if (floader_ && floader_->hasVertexFeatures()) {
+    // relabeled vertex -> its input id -> feature (src/core/gpu/data.cu:200-216)
+    res.verticesFeatures.assign((size_t)V, 0);
+    const int *U = eloader_->U().data(), *Vv = eloader_->V().data();
+    for (int64_t i = 0; i < E; i++) {
+      res.verticesFeatures[(size_t)res.Eg[3 * i]] = floader_->vertexFeature(U[beg + i]);
+      res.verticesFeatures[(size_t)res.Eg[3 * i + 1]] = floader_->vertexFeature(Vv[beg + i]);
+    }
+  }
   res.totalBytes = calc_total_bytes(res.numEdges, res.numVertices);
   if (cache) {
     const auto cpath = cacheGraphDirPath(beg, end);
@@ -260,6 +284,12 @@ struct GraphDataManagerImpl : GraphDataManager {
                                &gp),
               "GraphDataManager::moveAsync");
     s.graph = std::shared_ptr<evx_graph>(gp, [](evx_graph *p) { evx_graph_free(p); });
+    const bool vf = h.verticesFeatures.size() == h.numVertices && h.numVertices > 0;
+    const bool ef = h.edgeFeatures.size() == h.numEdges && h.numEdges > 0;
+    if (vf || ef)
+      check_evx(evx_graph_set_features(gp, vf ? h.verticesFeatures.data() : nullptr,
+                                       ef ? h.edgeFeatures.data() : nullptr),
+                "GraphDataManager::moveAsync(features)");
     s.device = device;
     s.name = h.name;
     s.beg = h.beg;
@@ -365,6 +395,9 @@ std::pair<int, int> GPUWorker::pause() { return {-1, -1}; }
 void GPUWorker::configure(long long, unsigned) {}
 void GPUWorker::setTuning(int, int, int, int, int) {}
 double GPUWorker::lastDeviceMs() const { return 0.0; }
+void GPUWorker::setConstraints(const evx_constraints *c) {
+  if (c) throw std::runtime_error("this worker takes no query constraints");
+}
 int GPUWorker::lastKernelLaunches() const { return 0; }
 
 GPUWorkerEVX::GPUWorkerEVX(int gpu, int sizeBlock) : GPUWorker("EVX", gpu, sizeBlock) {
@@ -372,6 +405,11 @@ GPUWorkerEVX::GPUWorkerEVX(int gpu, int sizeBlock) : GPUWorker("EVX", gpu, sizeB
 }
 
 GPUWorkerEVX::~GPUWorkerEVX() { evx_worker_destroy(w_); }
+
+void GPUWorkerEVX::setConstraints(const evx_constraints *c) {
+  hasCons_ = c != nullptr;
+  if (c) cons_ = *c;
+}
 
 void GPUWorkerEVX::configure(long long enumCap, unsigned flags) {
   enumCap_ = enumCap;
@@ -388,9 +426,14 @@ void GPUWorkerEVX::take(data::MineJob &job) {
   const data::DeviceJobData *d = job.data;
   if (!d || !d->graph) throw std::runtime_error("take: job without device data");
   k_ = (int)d->mu.size();
-  check_evx(evx_worker_take(w_, d->graph.get(), k_, d->mu.data(), d->mv.data(), job.delta, job.beg,
-                            job.end, enumCap_, flags_),
-            "take");
+  if (hasCons_)
+    check_evx(evx_worker_take_constrained(w_, d->graph.get(), k_, d->mu.data(), d->mv.data(), job.delta,
+                                          job.beg, job.end, enumCap_, flags_, &cons_),
+              "take");
+  else
+    check_evx(evx_worker_take(w_, d->graph.get(), k_, d->mu.data(), d->mv.data(), job.delta, job.beg,
+                              job.end, enumCap_, flags_),
+              "take");
   bound_ = true;
 }
 

@@ -6,6 +6,7 @@
 #include <pybind11/stl/filesystem.h>
 #include <pybind11/stl_bind.h>
 
+#include <cstring>
 #include <sstream>
 
 #include "corelib.h"
@@ -42,6 +43,9 @@ PYBIND11_MODULE(corelib, m) {
       .def_readonly("numEdges", &data::HostGraphData::numEdges)
       .def_readonly("numVertices", &data::HostGraphData::numVertices)
       .def_readonly("totalBytes", &data::HostGraphData::totalBytes)
+      .def_readonly("Eg", &data::HostGraphData::Eg)
+      .def_readonly("edgeFeatures", &data::HostGraphData::edgeFeatures)
+      .def_readonly("verticesFeatures", &data::HostGraphData::verticesFeatures)
       .def("__repr__", [](const data::HostGraphData &e) {
         std::ostringstream s;
         s << "<HostGraphData>\nname: " << e.name << "\nbeg: " << e.beg << ", end: " << e.end
@@ -96,6 +100,16 @@ PYBIND11_MODULE(corelib, m) {
       .def_readonly("name", &data::HostMotifData::name)
       .def_readonly("numEdges", &data::HostMotifData::numEdges)
       .def_readonly("numVertices", &data::HostMotifData::numVertices)
+      .def("motifEdges",
+           [](const data::HostMotifData &m) {
+             std::vector<int> mu, mv;
+             for (auto &e : m.edges) {
+               mu.push_back(e.u);
+               mv.push_back(e.v);
+             }
+             return std::make_pair(mu, mv);
+           },
+           "(sources, targets) of the relabeled motif edges")
       .def_property_readonly("edges", [](const data::HostMotifData &e) {
         std::vector<std::tuple<int, int, int>> r;
         for (auto &x : e.edges) r.emplace_back(x.u, x.v, x.t);
@@ -142,6 +156,23 @@ PYBIND11_MODULE(corelib, m) {
       .def("pause", &GPUWorker::pause)
       .def("printEnum", &GPUWorker::printEnum)
       .def("configure", &GPUWorker::configure, py::arg("enumCap"), py::arg("flags") = 0u)
+      .def(
+          "setConstraints",
+          [](GPUWorker &w, py::object blob) {
+            if (blob.is_none()) {
+              w.setConstraints(nullptr);
+              return;
+            }
+            const std::string s = blob.cast<py::bytes>();
+            if (s.size() != sizeof(evx_constraints))
+              throw std::invalid_argument("setConstraints: expected the " + std::to_string(sizeof(evx_constraints)) +
+                                          "-byte evx_constraints struct");
+            evx_constraints c;
+            std::memcpy(&c, s.data(), sizeof(c));
+            w.setConstraints(&c);
+          },
+          py::arg("constraints"),
+          "bytes of an evx_constraints struct (everest_b200.constraints), or None")
       .def("setTuning", &GPUWorker::setTuning)
       .def("lastDeviceMs", &GPUWorker::lastDeviceMs)
       .def("lastKernelLaunches", &GPUWorker::lastKernelLaunches)

@@ -511,7 +511,9 @@ int evx_graph_set_features(evx_graph *h, const int *node_features, const int *ed
 int evx_worker_take_constrained(evx_worker *w, const evx_graph *gh, int k, const int *mu, const int *mv,
                                 int delta, int64_t beg, int64_t end, int64_t enum_cap, unsigned flags,
                                 const evx_constraints *c) {
-  if (!c) return evx_worker_take(w, gh, k, mu, mv, delta, beg, end, enum_cap, flags);
+  // nothing to check: the plain search (the same matches, and its tuned kernel)
+  if (!c || (c->anti_mask == 0 && !c->has_temporal && c->node_mode == 0 && !c->has_edge && !c->has_filter))
+    return evx_worker_take(w, gh, k, mu, mv, delta, beg, end, enum_cap, flags);
   if (!w || !gh || !mu || !mv) return fail(EVX_ERR_INVALID, "null argument");
   if (gh->g.device != w->device) return fail(EVX_ERR_INVALID, "graph and worker on different devices");
   if (flags & ~EVX_FLAG_EXACT_TOTAL)

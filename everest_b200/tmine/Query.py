@@ -4,6 +4,11 @@
     graph: wiki-talk.txt       # temporal edge list (u v t lines)
     constraints:
       delta: 86400
+      node0: f > 500000000     # optional: node predicates (or `node` for all)
+      edge: f % 2 == 0         # optional: edge predicate
+      temporal: [900, 1800]    # optional: gap bound of each edge after the previous one
+      antiEdge: [False, False, True, False, False]   # optional: edges that must not exist
+      filter: (e0 + e1) > 100  # optional: over the matched edges' features
     options:
       gpu: 1
       enumerate: 1000          # optional: enumerate up to this many rows
@@ -11,8 +16,10 @@
       warpBalancing: True      # False disables work stealing
       tailExpansion: True      # False disables range-arithmetic tail counting
 
-Label, fine-grained temporal, anti-edge and filter constraints are not on
-this path and are rejected with NotImplementedError.
+The constraints are checked against the motif when the query runs
+(everest_b200.constraints.Constraints.from_yaml, which refuses what the
+reference's generated code cannot run); node and edge predicates and filters
+read the features of the random-feature file (EVX_RAND_FILE).
 """
 import os
 
@@ -21,7 +28,6 @@ import yaml
 from . import locations
 
 DEFAULT_OPTIONS = {"gpu": 1, "warpCentric": True, "warpBalancing": True, "tailExpansion": True}
-UNSUPPORTED = ("temporal", "antiEdge", "filter")
 
 
 class Options:
@@ -62,13 +68,22 @@ class Options:
 class Constraints:
     def __init__(self, cons):
         self.cons = dict(cons or {})
-        bad = [k for k in self.cons if k in UNSUPPORTED or k.startswith("node") or k.startswith("edge")]
-        if bad:
-            raise NotImplementedError(
-                f"constraints {bad} (labels, fine-grained temporal windows, anti-edges, filters) "
-                "are not supported by this miner; only 'delta' is")
         if "delta" not in self.cons:
             raise ValueError("query constraints need 'delta'")
+
+    def isTemporal(self) -> bool:
+        return "temporal" in self.cons
+
+    def isAnti(self) -> bool:
+        return "antiEdge" in self.cons
+
+    def isFilter(self) -> bool:
+        return "filter" in self.cons
+
+    def compile(self, mu, mv):
+        """The checked, compiled constraints for a motif (relabeled edges)."""
+        from ..constraints import Constraints as Compiled
+        return Compiled.from_yaml(self.cons, mu, mv)
 
     def isDelta(self) -> bool:
         return "delta" in self.cons

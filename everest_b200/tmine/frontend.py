@@ -53,6 +53,9 @@ class Mining:
         w = self.libManager.construct(self.libName, 0)
         opts = query.options()
         w.configure(opts.enumNum() if opts.enumerate() else 0, opts.flags())
+        mu, mv = hostMotif.motifEdges()
+        cons = query.constraints().compile(mu, mv)
+        w.setConstraints(None if cons.empty else bytes(cons.to_struct()))
         ex = self._execution()
         ex.setHostMotif(hostMotif)
         ex.setWorker(w)

@@ -53,6 +53,35 @@ def test_edge_list_loader_and_cache(tmp_path):
     assert part.numEdges == 800 and part.beg == 100 and part.end == 900
 
 
+def test_feature_loader_follows_the_reference_mapping(tmp_path):
+    """Edge i (time-sorted) takes rands[i]; the input vertex of rank r among
+    the distinct ids takes rands[r] (src/core/gpu/data.cu:57-79,200-216); a
+    relabeled vertex carries its input vertex's feature."""
+    spec = synth.GraphSpec("cl-feat", "zipf", 400, 3000, seed=4, t_max=9000)
+    u, v, t = synth.generate(spec)
+    u = u * 7 + 11  # sparse, unordered input ids
+    v = v * 7 + 11
+    p = tmp_path / "g.txt"
+    write_graph(p, u, v, t)
+    rands = np.random.default_rng(1).integers(-10**9, 10**9, u.size + 50).astype(np.int32)
+    rp = tmp_path / "rands.bin"
+    rands.tofile(rp)
+    e = core.data.EdgeListLoader(str(p))
+    f = core.data.FeatureLoader(e, str(rp))
+    ids = np.unique(np.concatenate([u, v]))
+    assert f.edgeFeaturesLength() == u.size and f.verticesFeaturesLength() == ids.size
+    hg = core.data.GraphDataLoader(e, f).createGraphData(0, 0, False)
+    assert np.array_equal(np.asarray(hg.edgeFeatures), rands[: u.size])
+    eg = np.asarray(hg.Eg).reshape(-1, 3)
+    vf = np.asarray(hg.verticesFeatures)
+    assert np.array_equal(vf[eg[:, 0]], rands[np.searchsorted(ids, u)])
+    assert np.array_equal(vf[eg[:, 1]], rands[np.searchsorted(ids, v)])
+    # a short file gives no vertex features
+    rands[:10].tofile(rp)
+    f2 = core.data.FeatureLoader(e, str(rp))
+    assert f2.edgeFeaturesLength() == 0 and f2.verticesFeaturesLength() == 0
+
+
 def divide_list_restated(T, delta, num):
     """src/core/cpu/data.cc:345-369 restated in Python."""
     size = len(T)

@@ -98,3 +98,37 @@ def test_legacy_corelib_flow(inputs):
     assert ex2.run(5000) == want
     assert core.allCount([w]) == want
     del w
+
+
+def test_constrained_query_end_to_end(tmp_path, monkeypatch):
+    """A YAML query with node predicates, temporal gaps, an anti-edge and a
+    filter, features from a random-feature file, through the tmine driver."""
+    from everest_b200.constraints import Constraints
+    spec = synth.GraphSpec("e2e-cons", "zipf", 500, 20_000, seed=23, t_max=200_000)
+    u, v, t = synth.generate(spec)
+    perm = np.random.default_rng(5).permutation(u.size)
+    synth.write_edge_text(str(tmp_path / "g.txt"), u[perm], v[perm], t[perm])
+    rands = np.random.default_rng(6).integers(0, 10, u.size + 10).astype(np.int32)
+    rands.tofile(tmp_path / "rands.bin")
+    (tmp_path / "M4-A.txt").write_text("1 2 1\n2 3 2\n3 1 3\n3 4 4\n4 1 5\n")
+    cons = {"delta": 20_000, "node0": "f > 2", "node1": "f < 8", "node2": "f > 1", "node3": "f != 5",
+            "antiEdge": [False, False, True, False, False], "temporal": [10_000, 15_000, 15_000, 10_000],
+            "filter": "(e0 + e1 + e3) > 6"}
+    q = tmp_path / "q.yaml"
+    q.write_text("pattern: M4-A.txt\ngraph: g.txt\nconstraints:\n"
+                 + "".join(f"  {k}: {v!r}\n" if isinstance(v, str) else f"  {k}: {v}\n" for k, v in cons.items())
+                 + "options:\n  gpu: 1\n")
+    monkeypatch.setenv("EVX_MOTIF_ROOT", str(tmp_path))
+    monkeypatch.setenv("EVX_GRAPH_ROOT", str(tmp_path))
+    monkeypatch.setenv("EVX_RAND_FILE", str(tmp_path / "rands.bin"))
+    cnt = frontend.MiningSingle(str(q)).run(out=lambda *a, **k: None)[0]
+    order = np.argsort(t[perm], kind="stable")
+    us, vs, ts = u[perm][order], v[perm][order], t[perm][order]
+    ids = np.unique(np.concatenate([u, v]))
+    V = int(ids.max()) + 1
+    nf = np.zeros(V, np.int32)
+    nf[ids] = rands[: ids.size]
+    mu, mv = [0, 1, 2, 2, 3], [1, 2, 0, 3, 0]
+    c = Constraints.from_yaml(cons, mu, mv).to_struct()
+    want = O.count_constrained(O.Graph(us, vs, ts, V), mu, mv, 20_000, c, nf, rands[: u.size])
+    assert cnt == want and want > 0

@@ -34,11 +34,20 @@ def test_query_enumerate_and_flags(tmp_path):
     assert o.flags() == 4 | 8
 
 
-def test_query_rejects_out_of_scope_constraints(tmp_path):
-    for cons in ("{delta: 5, temporal: [1, 2]}", "{delta: 5, node0: 'f > 3'}", "{delta: 5, antiEdge: [False]}",
-                 "{delta: 5, filter: 'e0 > 1'}", "{delta: 5, edge: 'f > 1'}"):
-        with pytest.raises(NotImplementedError):
-            Query.Query(write(tmp_path, "q.yaml", f"pattern: a\ngraph: b\nconstraints: {cons}\n"))
+def test_query_constraints_compile_against_the_motif(tmp_path):
+    q = Query.Query(write(tmp_path, "q.yaml", "pattern: a\ngraph: b\nconstraints: {delta: 5, temporal: [1, 2, 3], "
+                                             "antiEdge: [False, False, True, False], node: 'f > 3', "
+                                             "filter: 'e0 + e3 > 1'}\n"))
+    c = q.constraints()
+    assert c.isTemporal() and c.isAnti() and c.isFilter() and c.delta() == 5
+    st = c.compile([0, 1, 2, 2], [1, 2, 0, 3]).to_struct()
+    assert st.anti_mask == 4 and st.has_temporal and st.node_mode == 1 and st.has_filter
+    for cons, mu, mv in (("{delta: 5, edge0: 'f > 1'}", [0, 1], [1, 2]),
+                         ("{delta: 5, antiEdge: [False, True, False]}", [0, 1, 2], [1, 2, 0]),
+                         ("{delta: 5, label: 3}", [0, 1], [1, 2])):
+        q = Query.Query(write(tmp_path, "q1.yaml", f"pattern: a\ngraph: b\nconstraints: {cons}\n"))
+        with pytest.raises(ValueError):
+            q.constraints().compile(mu, mv)
     with pytest.raises(ValueError):
         Query.Query(write(tmp_path, "q2.yaml", "pattern: a\ngraph: b\nconstraints: {}\n"))
 
