@@ -24,5 +24,6 @@ def dynLibPath() -> str:
 
 
 def randFilePath() -> str:
-    """Random-feature file; labels are not on this path, a missing file is fine."""
+    """Random-feature file (raw int32; the reference hard-codes its path): node /
+    edge predicates and filters read it; queries without them need none."""
     return os.environ.get("EVX_RAND_FILE", "")
