@@ -57,6 +57,9 @@ struct CacheDirectoryAccess {
   std::filesystem::path cacheVPath() const { return cacheDir_ / "V.cache"; }
   std::filesystem::path cacheTPath() const { return cacheDir_ / "T.cache"; }
   std::filesystem::path cacheIDSPath() const { return cacheDir_ / "IDS.cache"; }
+  std::filesystem::path cacheFEPath() const { return cacheDir_ / "EdgesFeatures"; }
+  std::filesystem::path cacheFVVPath() const { return cacheDir_ / "VerticesFeaturesValue"; }
+  std::filesystem::path cacheFVMPath() const { return cacheDir_ / "VerticesFeaturesMap"; }
   std::filesystem::path cacheGraphDirPath(size_t beg, size_t end) const;
   std::string name() const { return name_; }
 };
@@ -79,8 +82,11 @@ class EdgeListLoader : public CacheDirectoryAccess {
 // Random per-edge / per-vertex features (src/core/cpu/data.cc:316-343,
 // src/core/gpu/data.cu:57-79): a raw int32 file whose first E values are the
 // features of the time-sorted edges and whose first N values those of the N
-// distinct vertex ids in ascending order.  A missing or short file yields
-// empty features (queries without node / edge predicates need none).
+// distinct vertex ids in ascending order.  Like the reference, the derived
+// arrays are cached beside the edge-list cache (EdgesFeatures,
+// VerticesFeaturesValue, VerticesFeaturesMap) and read from there when all
+// three exist.  A missing or short file yields empty features (queries
+// without node / edge predicates need none).
 class FeatureLoader : public CacheDirectoryAccess {
  public:
   FeatureLoader(const EdgeListLoader *eloader, const std::filesystem::path &pathToRands);

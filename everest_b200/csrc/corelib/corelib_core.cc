@@ -96,11 +96,21 @@ EdgeListLoader::EdgeListLoader(const std::filesystem::path &pathToGraph, bool us
 
 FeatureLoader::FeatureLoader(const EdgeListLoader *eloader, const std::filesystem::path &pathToRands)
     : CacheDirectoryAccess(eloader->graphPath_, false) {
+  const size_t E = eloader->edgeListLength();
+  // the reference's feature caches (src/core/cpu/data.cc:316-327)
+  std::vector<int> fe, fvv, fvm;
+  if (read_ints(cacheFEPath(), fe) && read_ints(cacheFVVPath(), fvv) && read_ints(cacheFVMPath(), fvm) &&
+      fvv.size() == fvm.size() && std::is_sorted(fvm.begin(), fvm.end())) {
+    if (fe.size() >= E) edge_.assign(fe.begin(), fe.begin() + (long)E);
+    vertex_ = std::move(fvv);
+    vertexIds_ = std::move(fvm);
+    return;
+  }
   std::vector<int> r;
   if (pathToRands.empty() || !read_ints(pathToRands, r)) return;
-  const size_t E = eloader->edgeListLength();
   if (r.size() >= E) edge_.assign(r.begin(), r.begin() + (long)E);
   // distinct vertex ids, ascending; vertex i of that order takes value i
+  // (src/core/gpu/data.cu:57-79)
   std::vector<int> ids(eloader->U());
   ids.insert(ids.end(), eloader->V().begin(), eloader->V().end());
   std::sort(ids.begin(), ids.end());
@@ -108,6 +118,11 @@ FeatureLoader::FeatureLoader(const EdgeListLoader *eloader, const std::filesyste
   if (r.size() >= ids.size()) {
     vertex_.assign(r.begin(), r.begin() + (long)ids.size());
     vertexIds_ = std::move(ids);
+  }
+  if (edge_.size() == E && !vertex_.empty() && std::filesystem::exists(cacheDir_)) {
+    write_ints(cacheFEPath(), edge_);
+    write_ints(cacheFVVPath(), vertex_);
+    write_ints(cacheFVMPath(), vertexIds_);
   }
 }
 

@@ -76,9 +76,22 @@ def test_feature_loader_follows_the_reference_mapping(tmp_path):
     vf = np.asarray(hg.verticesFeatures)
     assert np.array_equal(vf[eg[:, 0]], rands[np.searchsorted(ids, u)])
     assert np.array_equal(vf[eg[:, 1]], rands[np.searchsorted(ids, v)])
-    # a short file gives no vertex features
+    # the reference's feature caches, written beside the edge-list cache ...
+    cdir = tmp_path / "g"
+    assert np.array_equal(np.fromfile(cdir / "EdgesFeatures", np.int32), rands[: u.size])
+    assert np.array_equal(np.fromfile(cdir / "VerticesFeaturesValue", np.int32), rands[: ids.size])
+    assert np.array_equal(np.fromfile(cdir / "VerticesFeaturesMap", np.int32), ids)
+    # ... and read back without the random-feature file
+    f3 = core.data.FeatureLoader(e, "")
+    hg3 = core.data.GraphDataLoader(e, f3).createGraphData(0, 0, False)
+    assert np.array_equal(np.asarray(hg3.verticesFeatures), vf)
+    assert np.array_equal(np.asarray(hg3.edgeFeatures), rands[: u.size])
+    # a short file (and no cache) gives no features
+    (tmp_path / "b").mkdir()
+    write_graph(tmp_path / "b" / "g.txt", u, v, t)
+    eb = core.data.EdgeListLoader(str(tmp_path / "b" / "g.txt"))
     rands[:10].tofile(rp)
-    f2 = core.data.FeatureLoader(e, str(rp))
+    f2 = core.data.FeatureLoader(eb, str(rp))
     assert f2.edgeFeaturesLength() == 0 and f2.verticesFeaturesLength() == 0
 
 
