@@ -47,6 +47,7 @@ class Request:
     flags: int = 0
     beg: int = 0          # root edge ids [beg, end); end < 0 = to the last root
     end: int = -1
+    constraints: Optional[object] = None  # compiled everest_b200.constraints.Constraints
     submitted: float = field(default_factory=time.perf_counter)
     future: Future = field(default_factory=Future)
 
@@ -122,20 +123,34 @@ class Server:
         self.thread.start()
 
     # ------------------------------------------------------------- API --
-    def add_graph(self, name: str, host: capi.HostGraph) -> None:
-        self.graphs[name] = self.be.DeviceGraph(host, self.device)
+    def add_graph(self, name: str, host: capi.HostGraph, node_features=None, edge_features=None) -> None:
+        """Make a graph resident; node features (per relabeled vertex) and
+        edge features (per sorted edge) serve constrained queries."""
+        g = self.be.DeviceGraph(host, self.device)
+        if node_features is not None or edge_features is not None:
+            g.set_features(node_features, edge_features)
+        self.graphs[name] = g
 
     def submit(self, graph: str, mu, mv, delta: int, enum_cap: int = 0, flags: int = 0, beg: int = 0,
-               end: int = -1) -> Future:
+               end: int = -1, constraints=None) -> Future:
         """Queue a query; roots are the edge ids [beg, end) (the whole graph
-        by default), as in the reference's MineJob(data, delta, beg, end)."""
+        by default), as in the reference's MineJob(data, delta, beg, end).
+        constraints: the YAML constraint keys (a dict) or a compiled
+        everest_b200.constraints.Constraints; a constrained query runs on a
+        worker slot, like an enumeration."""
         if graph not in self.graphs:
             raise KeyError(f"graph {graph!r} is not resident")
-        r = Request(graph, list(mu), list(mv), int(delta), int(enum_cap), int(flags), int(beg), int(end))
+        if isinstance(constraints, dict):
+            from .constraints import Constraints
+            constraints = Constraints.from_yaml(constraints, list(mu), list(mv))
+        if constraints is not None and constraints.empty:
+            constraints = None
+        r = Request(graph, list(mu), list(mv), int(delta), int(enum_cap), int(flags), int(beg), int(end),
+                    constraints)
         with self.cv:
             if self.first_submit is None:
                 self.first_submit = r.submitted
-            (self.enum_q if enum_cap > 0 else self.count_q).append(r)
+            (self.enum_q if (enum_cap > 0 or constraints is not None) else self.count_q).append(r)
             self.cv.notify()
         return r.future
 
@@ -202,12 +217,13 @@ class Server:
         for i, w in enumerate(self.enum_workers):
             r = self.enum_reqs[i]
             if r is not None and w.done():
-                self.launch_log.append(("enumerate", self.enum_t0[i], time.perf_counter(), 1))
+                kind = "enumerate" if r.enum_cap > 0 else "constrained"
+                self.launch_log.append((kind, self.enum_t0[i], time.perf_counter(), 1))
                 try:
                     c, lim = w.result(), False
                 except capi.LimitExceeded:
                     c, lim = None, True
-                rows = w.enum_rows(r.enum_cap)
+                rows = w.enum_rows(r.enum_cap) if r.enum_cap > 0 else None
                 self.enum_reqs[i] = None
                 self._finish(r, Result(c, rows, limited=lim))
                 progressed = True
@@ -261,7 +277,11 @@ class Server:
             with self.lock:
                 self.enum_q.popleft()
                 self.enum_reqs[i] = r  # claimed under the lock (see the batches above)
-            w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags)
+            if r.constraints is not None:
+                w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags,
+                       constraints=r.constraints)
+            else:
+                w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags)
             if self.enum_blocks_per_sm and hasattr(w, "set_tuning"):
                 busy = bool(self.count_q) or any(x is not None for x in self.batch_reqs)
                 w.set_tuning(block=128, blocks_per_sm=self.enum_blocks_per_sm if busy else 0, roots_per_fetch=32,

@@ -337,7 +337,8 @@ EVX_API int evx_graph_set_features(evx_graph *g, const int *node_features, const
  * an anti-edge, and enumeration with anti-edges (its rows would name no
  * edge); node / edge predicates need the matching features on the graph.
  * Flags: EVX_FLAG_EXACT_TOTAL only.  The plain search's launch, result and
- * rows calls then run this job. */
+ * rows calls then run this job; the work limit (evx_worker_set_limit) does
+ * not apply to it.  A struct with no constraint set runs the plain search. */
 EVX_API int evx_worker_take_constrained(evx_worker *w, const evx_graph *g, int k, const int *mu,
                                         const int *mv, int delta, int64_t beg, int64_t end,
                                         int64_t enum_cap, unsigned flags, const evx_constraints *c);

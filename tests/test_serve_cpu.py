@@ -22,6 +22,8 @@ class FakeBackend:
         self.running_enum = 0
         self.enum_bps = []  # blocks per SM asked for at each enumeration launch
         self.batch_s = 0.002  # how long a launched batch takes
+        self.features = {}    # name -> (node features, edge features)
+        self.constrained = 0  # constrained launches
 
     def device_mem_info(self, device):
         with self.lock:
@@ -78,8 +80,9 @@ class FakeBackend:
             def set_tuning(self, block, blocks_per_sm, roots_per_fetch, steal_interval, min_split):
                 be.enum_bps.append(blocks_per_sm)
 
-            def take(self, g, mu, mv, d, beg, end, cap, flags):
+            def take(self, g, mu, mv, d, beg, end, cap, flags, constraints=None):
                 self.args = (g, mu, mv, d, cap)
+                self.cons = constraints
 
             def launch(self):
                 g, mu, mv, d, cap = self.args
@@ -87,7 +90,13 @@ class FakeBackend:
                     be.free -= cap * len(mu) * 4
                     be.running_enum += 1
                     be.max_concurrent_enum = max(be.max_concurrent_enum, be.running_enum)
-                self.rows, self.total = O.enumerate_rows(be.graphs[g], mu, mv, d, cap)
+                if self.cons is not None:
+                    nf, ef = be.features[g]
+                    be.constrained += 1
+                    self.total = O.count_constrained(be.graphs[g], mu, mv, d, self.cons.to_struct(), nf, ef)
+                    self.rows = None
+                else:
+                    self.rows, self.total = O.enumerate_rows(be.graphs[g], mu, mv, d, cap)
                 self.t_done = time.perf_counter() + 0.003
 
             def done(self):
@@ -196,4 +205,30 @@ def test_enumerations_share_the_gpu_only_beside_count_work(graph):
     srv.drain(60)
     assert all(f.result(1) is not None for f in futs)
     assert be.enum_bps[0] == 2 and be.enum_bps[-1] == 0
+    srv.close()
+
+
+def test_constrained_queries_run_on_worker_slots(graph):
+    be = FakeBackend({"g": graph}, free_bytes=1 << 40)
+    rng = np.random.Generator(np.random.PCG64(3))
+    be.features["g"] = (rng.integers(0, 10, graph.V).astype(np.int32),
+                        rng.integers(0, 10, graph.E).astype(np.int32))
+    srv = serve.Server(max_batch=8, inflight_batches=2, enum_slots=2, mem_reserve=0, backend=be)
+    srv.add_graph("g", "g")
+    cons = [({"node": "f > 3"}, [0, 1, 2], [1, 2, 0], 3000),
+            ({"temporal": [800, 400], "edge": "f % 3 != 0"}, [0, 0, 0], [1, 2, 3], 2000),
+            ({"antiEdge": [False, False, True, False], "filter": "e0 + e3 > 8"}, [0, 1, 1, 2], [1, 2, 0, 0], 4000),
+            ({}, [0, 1], [1, 0], 4000)]  # no constraint: a plain batched count
+    futs = [srv.submit("g", mu, mv, d, constraints=c) for c, mu, mv, d in cons]
+    plain = srv.submit("g", [0, 1, 2], [1, 2, 0], 3000)
+    srv.drain(60)
+    from everest_b200.constraints import Constraints
+    nf, ef = be.features["g"]
+    for (c, mu, mv, d), f in zip(cons, futs):
+        want = O.count_constrained(graph, mu, mv, d, Constraints.from_yaml(c, mu, mv).to_struct(), nf, ef)
+        res = f.result(1)
+        assert res.count == want and res.rows is None
+    assert plain.result(1).count == O.count(graph, [0, 1, 2], [1, 2, 0], 3000)[0]
+    assert be.constrained == 3  # the empty set went to a batch
+    assert any(k == "constrained" for k, *_ in srv.launch_log)
     srv.close()
