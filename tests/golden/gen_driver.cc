@@ -11,7 +11,7 @@
 extern "C" int gen_count(const int *eg, int numeg, const int *in_v, const int *in_r,
                          const int *out_v, const int *out_r, const int *node_feat,
                          const int *edge_feat, const int *mu, const int *mv, int k, int delta,
-                         int work, unsigned long long *count_out) {
+                         int work, int *rows, const int *euid, unsigned long long *count_out) {
   std::vector<corelib::MotifEdgeInfoV1> mi;
   int node_max = 1;
   for (int i = 1; i < k; i++) {
@@ -34,8 +34,14 @@ extern "C" int gen_count(const int *eg, int numeg, const int *in_v, const int *i
   const corelib::TemporalEdge *Eg = reinterpret_cast<const corelib::TemporalEdge *>(eg);
   for (int tid = 0; tid < work; tid++) {
     gen_block_idx.x = (unsigned)tid;
+#ifdef GEN_ENUM
+    // rows of Euid (here the sorted edge ids) into rows[cap * k]
+    MotifMatching_dispatch(work, delta, Eg, numeg, in_v, in_r, out_v, out_r, node_feat, edge_feat,
+                           mi.data(), k, rows, euid, &gcount);
+#else
     MotifMatching_dispatch(work, delta, Eg, numeg, in_v, in_r, out_v, out_r, node_feat, edge_feat,
                            mi.data(), k, &gcount);
+#endif
   }
   *count_out = gcount;
   return 0;

@@ -36,3 +36,9 @@ template <class T> static inline T __shfl_down_sync(unsigned, T, int) { return T
 static inline unsigned long long atomicAdd(unsigned long long *p, unsigned long long v) {
   return __atomic_fetch_add(p, v, __ATOMIC_RELAXED);
 }
+// The enumeration body stops the warp-centric root dispatcher with
+// atomicExch(source, work) once the cap is reached; with one root per thread
+// there is no dispatcher, so the fixtures keep every total under the cap.
+static int gen_source_word = 0;
+static int *source = &gen_source_word;
+static inline int atomicExch(int *p, int v) { return __atomic_exchange_n(p, v, __ATOMIC_RELAXED); }

@@ -52,6 +52,17 @@ MOTIFS = {
 ANTI = {"M4-A": [False, False, True, False, False],
         "anti2": [False, False, True, True, False, False],
         "anti-fan": [False, False, True, False, False]}
+ENUM_CAP = 50_000
+ENUM_CASES = [
+    ("dense-4", "tri", {"node": "f > 3"}),
+    ("mid-hub", "tri", {"node": "f > 3"}),
+    ("mid-hub", "rep3", {"temporal": [500, 300], "edge": "f % 3 != 1"}),
+    ("mid-hub", "M4", {"node0": "f % 2 == 0", "node1": "f < 7", "node2": "f != 3", "node3": "f >= 2"}),
+    ("mid-hub", "tri", {"node": "f > 2", "temporal": [600, 300], "filter": "e0 * e1 > 10"}),
+    ("mid-ties", "star3", {"node": "f > 3"}),
+    ("zipf-2k-10k", "star3", {"node": "f > 2", "temporal": [120000, 60000], "filter": "e0 * e1 > 10"}),
+    ("mid-uniform", "star3", {"filter": "e0 + e1 > 9"}),
+]
 PER_NODE = ["f % 2 == 0", "f < 7", "f != 3", "f >= 2", "(f & 1) || f > 5"]
 
 
@@ -88,15 +99,16 @@ def load_kernelgen(scratch):
     return KG, Q
 
 
-def render(KG, Q, scratch, mu, mv, cons):
+def render(KG, Q, scratch, mu, mv, cons, enum_cap=0):
     motif = os.path.join(scratch, "motif.txt")
     with open(motif, "w") as f:
         for i, (a, b) in enumerate(zip(mu, mv)):
             f.write(f"{a + 1} {b + 1} {i + 1}\n")
     q = Q.Query.__new__(Q.Query)
-    q.queryFile = {"pattern": motif, "graph": "-", "constraints": cons,
-                   "options": {"gpu": 1, "warpCentric": False, "warpBalancing": False,
-                               "tailExpansion": False}}
+    opts = {"gpu": 1, "warpCentric": False, "warpBalancing": False, "tailExpansion": False}
+    if enum_cap:
+        opts["enumerate"] = enum_cap
+    q.queryFile = {"pattern": motif, "graph": "-", "constraints": cons, "options": opts}
     q.name = "fixture"
     q.cons = Q.Constraints(cons)
     opts = Q.Options()
@@ -114,17 +126,18 @@ def render(KG, Q, scratch, mu, mv, cons):
     return "\n".join(body) + "\n"
 
 
-def build_lib(scratch, body, tag):
+def build_lib(scratch, body, tag, enum=False):
     inc = os.path.join(scratch, f"body_{tag}.inc")
     with open(inc, "w") as f:
         f.write(body)
     so = os.path.join(scratch, f"gen_{tag}.so")
     subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-w", "-fpermissive", f"-I{HERE}",
-                    f'-DGEN_BODY="{inc}"', "-o", so, os.path.join(HERE, "gen_driver.cc")], check=True)
+                    f'-DGEN_BODY="{inc}"'] + (["-DGEN_ENUM"] if enum else []) +
+                   ["-o", so, os.path.join(HERE, "gen_driver.cc")], check=True)
     L = ctypes.CDLL(so)
     ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
     L.gen_count.argtypes = [ip, ctypes.c_int, ip, ip, ip, ip, ip, ip, ip, ip, ctypes.c_int,
-                            ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong)]
+                            ctypes.c_int, ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_ulonglong)]
     L.gen_count.restype = ctypes.c_int
     return L
 
@@ -153,7 +166,7 @@ def main():
                     out = ctypes.c_ulonglong(0)
                     L.gen_count(eg, g.E, g.in_eid, g.in_off, g.out_eid, g.out_off, nf, ef,
                                 np.asarray(mu, np.int32), np.asarray(mv, np.int32), k, delta, work,
-                                ctypes.byref(out))
+                                np.zeros(1, np.int32), np.zeros(1, np.int32), ctypes.byref(out))
                     ref = int(out.value)
                     c = Constraints.from_yaml(cons, mu, mv).to_struct()
                     mine = O.count_constrained(g, mu, mv, delta, c, nf, ef)
@@ -162,11 +175,40 @@ def main():
                     cases.append({"graph": gname, "motif": mname, "mu": mu, "mv": mv, "delta": delta,
                                   "constraints": cons, "count": ref})
                     print(f"{gname:12s} {mname:8s} {ref:10d} {sorted(k for k in cons if k != 'delta')}")
+        # enumeration: the generated enumeration body's rows (Euid = sorted
+        # edge id here) against the oracle's, every total under the cap
+        enum_cases = []
+        for gname, mname, cons in ENUM_CASES:
+            g = O.Graph(d[gname + "_u"], d[gname + "_v"], d[gname + "_t"], int(d[gname + "_V"][0]))
+            nf, ef = feats[gname + "_node"], feats[gname + "_edge"]
+            mu, mv = MOTIFS[mname]
+            k = len(mu)
+            cons = dict(cons, delta=GRAPHS[gname])
+            L = build_lib(scratch, render(KG, Q, scratch, mu, mv, cons, ENUM_CAP), tag, enum=True)
+            tag += 1
+            eg = np.stack([g.u, g.v, g.t], axis=1).astype(np.int32).ravel()
+            rows = np.zeros(ENUM_CAP * k, np.int32)
+            out = ctypes.c_ulonglong(0)
+            L.gen_count(eg, g.E, g.in_eid, g.in_off, g.out_eid, g.out_off, nf, ef, np.asarray(mu, np.int32),
+                        np.asarray(mv, np.int32), k, GRAPHS[gname], max(0, g.E - k + 1), rows,
+                        np.arange(max(g.E, 1), dtype=np.int32), ctypes.byref(out))
+            total = int(out.value)
+            if not 0 < total < ENUM_CAP:
+                raise SystemExit(f"enumeration case {gname} {mname} {cons}: total {total}")
+            ref_rows = sorted(map(tuple, rows[: total * k].reshape(total, k).tolist()))
+            c = Constraints.from_yaml(cons, mu, mv).to_struct()
+            o_rows, o_total = O.enumerate_constrained(g, mu, mv, GRAPHS[gname], c, ENUM_CAP, nf, ef)
+            if o_total != total or sorted(map(tuple, o_rows.tolist())) != ref_rows:
+                raise SystemExit(f"oracle rows differ from the reference's: {gname} {mname} {cons}")
+            enum_cases.append({"graph": gname, "motif": mname, "mu": mu, "mv": mv, "delta": GRAPHS[gname],
+                               "constraints": cons, "total": total, "rows": [list(r) for r in ref_rows]})
+            print(f"enumerate {gname:12s} {mname:8s} {total:6d} rows")
     np.savez_compressed(os.path.join(HERE, "constraint_features.npz"), **feats)
     with open(os.path.join(HERE, "constraint_golden.json"), "w") as f:
         json.dump({"source": "reference KernelGen output (warp options off) run on the host; "
                              "oracle/evx_oracle_cons.c agrees on every case",
-                   "features": "constraint_features.npz", "cases": cases}, f, indent=0)
+                   "features": "constraint_features.npz", "cases": cases, "enum_cases": enum_cases},
+                  f, indent=0)
     print(len(cases), "cases")
 
 

@@ -158,3 +158,17 @@ def test_constraint_checks():
     with pytest.raises(ConstraintError, match="no earlier real edge"):
         Constraints.from_yaml({"delta": 1, "antiEdge": [False, False, True, False]},
                               [0, 1, 1, 2], [1, 2, 3, 0])
+
+
+def test_oracle_rows_match_reference_generated_enumeration():
+    """The generated enumeration body's rows (Euid of e_0 .. e_{k-1}, here
+    the sorted edge ids) equal the oracle's, as multisets."""
+    gs = _graphs()
+    cases = _golden()["enum_cases"]
+    assert len(cases) >= 8
+    for c in cases:
+        g, nf, ef = gs[c["graph"]]
+        cons = Constraints.from_yaml(c["constraints"], c["mu"], c["mv"]).to_struct()
+        rows, total = O.enumerate_constrained(g, c["mu"], c["mv"], c["delta"], cons, c["total"] + 5, nf, ef)
+        assert total == c["total"]
+        assert sorted(map(tuple, rows.tolist())) == [tuple(r) for r in c["rows"]], c["motif"]
