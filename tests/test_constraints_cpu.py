@@ -172,3 +172,101 @@ def test_oracle_rows_match_reference_generated_enumeration():
         rows, total = O.enumerate_constrained(g, c["mu"], c["mv"], c["delta"], cons, c["total"] + 5, nf, ef)
         assert total == c["total"]
         assert sorted(map(tuple, rows.tolist())) == [tuple(r) for r in c["rows"]], c["motif"]
+
+
+def _brute(u, v, t, mu, mv, delta, anti, gaps, node_ok, edge_ok, filt, ef):
+    """Direct restatement of the documented semantics over all increasing
+    tuples of real edges (tiny graphs only)."""
+    import itertools
+    k, E = len(mu), len(u)
+    real = [j for j in range(k) if not anti[j]]
+    prev = {}
+    for j in range(1, k):
+        p = j - 1
+        while p > 0 and anti[p]:
+            p -= 1
+        prev[j] = p
+
+    def window(j, e):  # e: motif edge -> edge id of the real ones
+        t0 = t[e[0]]
+        if gaps is None:
+            return t0 + delta
+        w = t[e[prev[j]]] + gaps[j - 1]
+        return w if j == 1 else min(w, t0 + delta)
+
+    total = 0
+    for tup in itertools.combinations(range(E), len(real)):
+        e = dict(zip(real, tup))
+        if u[e[0]] == v[e[0]]:
+            continue
+        phi, ok = {}, True
+        for j in real:
+            for a, x in ((mu[j], u[e[j]]), (mv[j], v[e[j]])):
+                if phi.setdefault(a, x) != x:
+                    ok = False
+        if not ok or len(set(phi.values())) != len(phi):
+            continue
+        if not all(node_ok(a, x) for a, x in phi.items()) or not all(edge_ok(e[j]) for j in real):
+            continue
+        if not all(t[e[j]] <= window(j, e) for j in real if j > 0):
+            continue
+        dead = False
+        for j in range(1, k):
+            if anti[j]:
+                tl = window(j, e)
+                if any(x > e[prev[j]] and t[x] <= tl and u[x] == phi[mu[j]] and v[x] == phi[mv[j]] and edge_ok(x)
+                       for x in range(E)):
+                    dead = True
+        if dead or (filt is not None and not filt([ef[e[j]] if j in e else 0 for j in range(k)])):
+            continue
+        total += 1
+    return total
+
+
+def test_oracle_matches_brute_force_semantics():
+    """The semantics written in include/everest_b200.h, restated as a
+    brute-force check, give the oracle's counts on random tiny graphs."""
+    rng = np.random.Generator(np.random.PCG64(99))
+    motifs = [([0, 1, 2], [1, 2, 0], [False] * 3), ([0, 1, 0], [1, 0, 1], [False] * 3),
+              ([0, 1, 2, 2, 3], [1, 2, 0, 3, 0], [False, False, True, False, False]),
+              ([0, 1, 1, 0, 2], [1, 2, 0, 2, 0], [False, False, True, False, False]),
+              ([0, 1, 2, 1, 2, 3], [1, 2, 0, 0, 3, 0], [False, False, True, True, False, False]),
+              ([0, 1], [1, 2], [False, False]), ([0, 0, 1], [1, 2, 2], [False] * 3)]
+    checked = 0
+    for trial in range(200):
+        E, V = int(rng.integers(8, 22)), int(rng.integers(3, 6))
+        u = rng.integers(0, V, E).astype(np.int32)
+        v = rng.integers(0, V, E).astype(np.int32)
+        t = np.sort(rng.integers(0, 12, E)).astype(np.int32)
+        nf = rng.integers(0, 4, V).astype(np.int32)
+        ef = rng.integers(0, 4, E).astype(np.int32)
+        mu, mv, anti = motifs[trial % len(motifs)]
+        k, n = len(mu), max(max(mu), max(mv)) + 1
+        delta = int(rng.integers(2, 10))
+        cons = {"delta": delta}
+        if any(anti):
+            cons["antiEdge"] = anti
+        gaps = None
+        if trial % 2:
+            gaps = [int(x) for x in rng.integers(0, 12, k - 1)]
+            cons["temporal"] = gaps
+        th = [int(x) for x in rng.integers(0, 3, n)]
+        if trial % 3 == 0:
+            cons.update({f"node{a}": f"f >= {th[a]}" for a in range(n)})
+        if trial % 4 == 1:
+            cons["edge"] = "f != 2"
+        real = [j for j in range(k) if not anti[j]]
+        filt = None
+        if trial % 5 == 2:
+            cons["filter"] = " + ".join(f"e{j}" for j in real) + f" > {len(real)}"
+            filt = lambda vals: sum(vals[j] for j in real) > len(real)  # noqa: E731
+        node_ok = (lambda a, x: nf[x] >= th[a]) if trial % 3 == 0 else (lambda a, x: True)
+        edge_ok = (lambda x: ef[x] != 2) if trial % 4 == 1 else (lambda x: True)
+        want = _brute(u, v, t, mu, mv, delta, anti, gaps, node_ok, edge_ok, filt, ef)
+        g = O.Graph(u, v, t, V)
+        c = Constraints.from_yaml(cons, mu, mv).to_struct()
+        roots = (0, max(0, E - k + 1))
+        got = O.count_constrained(g, mu, mv, delta, c, nf, ef, roots=roots)
+        assert got == want, (trial, cons, got, want)
+        checked += want > 0
+    assert checked > 40
