@@ -83,3 +83,33 @@ def serve_queries(window: int = 100_000, n: int = 10_000) -> List[dict]:
     with a cap log-uniform in [1e4, 1e6]."""
     graphs = [(synth.SPECS[k].name, synth.SPECS[k].num_edges) for k in ("bursty-1.1m-7.8m", "bursty-6m-63m")]
     return mixed_queries(n, 5, (3, 5), (2, 4), graphs, window, delta_range=(600, 604800), enum_frac=0.2)
+
+
+CONSTRAINED_DELTA = 86400
+
+
+def constrained_queries() -> List[Tuple[str, List[int], List[int], dict]]:
+    """The reference's additional-features query shapes
+    (system/queries/additional-features/*-M4-{no,v,t,all,f}.yaml) as
+    (name, mu, mv, constraints) on the 7.8M-edge graph with node and edge
+    features uniform in [0, 1e9): the reference's delta 3600 and gaps
+    900 / 1800 are scaled by 24 (delta 86400).  The "-f" filter names e0, e1,
+    e3: the reference's own names the anti-edge e2, which it reads past its
+    arrays."""
+    m4, m4a = ([0, 1, 2, 3], [1, 2, 3, 0]), ([0, 1, 2, 2, 3], [1, 2, 0, 3, 0])
+    nodes = {"node0": "f > 500000000", "node1": "f < 500000000", "node2": "f > 500000000",
+             "node3": "f < 500000000"}
+    anti = {"antiEdge": [False, False, True, False, False], "temporal": [21600, 43200, 43200, 21600]}
+    d = {"delta": CONSTRAINED_DELTA}
+    return [("M4-no", *m4, dict(d)), ("M4-v", *m4, dict(d, **nodes)),
+            ("M4-t", *m4, dict(d, temporal=[21600, 43200, 21600], **nodes)),
+            ("M4-all", *m4a, dict(d, **nodes, **anti)),
+            ("M4-f", *m4a, dict(d, filter="(e0 + e1 + e3) > 1000000000", **nodes, **anti))]
+
+
+def constrained_features(num_vertices: int, num_edges: int, seed: int = 5):
+    """Node features per input vertex id and edge features per sorted edge,
+    uniform in [0, 1e9)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return (rng.integers(0, 10**9, num_vertices).astype(np.int32),
+            rng.integers(0, 10**9, num_edges).astype(np.int32))

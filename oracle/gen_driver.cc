@@ -1,9 +1,13 @@
-// Runs one generated search body (GEN_BODY, extracted by
-// make_constraint_golden.py) over every root on the host.
+// Runs one generated search body (GEN_BODY, extracted by ref_generated.py)
+// over every root on the host, one OpenMP iteration per root (one CUDA
+// thread of the reference's grid).  TEST INFRASTRUCTURE ONLY.
 #include "gen_shim.h"
 #include GEN_BODY
 
 #include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 // Motif info as HostMotifData builds it (src/core/cpu/data.cc:411-449) and
 // DeviceJobData binds it (src/core/gpu/data.cu:516-526); motif nodes are
@@ -11,7 +15,8 @@
 extern "C" int gen_count(const int *eg, int numeg, const int *in_v, const int *in_r,
                          const int *out_v, const int *out_r, const int *node_feat,
                          const int *edge_feat, const int *mu, const int *mv, int k, int delta,
-                         int work, int *rows, const int *euid, unsigned long long *count_out) {
+                         int work, int *rows, const int *euid, int nthreads,
+                         unsigned long long *count_out) {
   std::vector<corelib::MotifEdgeInfoV1> mi;
   int node_max = 1;
   for (int i = 1; i < k; i++) {
@@ -32,6 +37,10 @@ extern "C" int gen_count(const int *eg, int numeg, const int *in_v, const int *i
   }
   unsigned long long gcount = 0;
   const corelib::TemporalEdge *Eg = reinterpret_cast<const corelib::TemporalEdge *>(eg);
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+#endif
   for (int tid = 0; tid < work; tid++) {
     gen_block_idx.x = (unsigned)tid;
 #ifdef GEN_ENUM

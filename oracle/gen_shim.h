@@ -1,8 +1,8 @@
 // Host shim for the search kernel the reference generates per query
 // (system/tmine/KernelGen.py with warpCentric, warpBalancing and
 // tailExpansion off, so each CUDA thread is one root's sequential search).
-// Used only by make_constraint_golden.py to produce fixtures: the
-// generated body is compiled for the host against these stand-ins.
+// TEST INFRASTRUCTURE ONLY (oracle/ref_generated.py): the generated body is
+// compiled for the host against these stand-ins.
 #pragma once
 #include <algorithm>
 #include <cstdint>

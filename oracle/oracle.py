@@ -7,6 +7,9 @@ never imports this module.
 
 * ``liboracle.so`` (``evx_oracle.c``): C restatement of the reference's
   count / enumerate semantics, instrumented for the algorithmic-bytes model.
+* ``_ref/gen_<query>.so``: the search the reference generates per query
+  (KernelGen, warp options off), built for the host by ``ref_generated.py``
+  for the constrained bench queries.
 * ``_ref/libref_baseline.so``: the reference's own legacy Baseline search body
   (``plugins/GPUWorkerBaseline.cu:21-206``) compiled for the host by
   ``ref_baseline.mk``; present only where the reference tree was available at
@@ -54,6 +57,10 @@ def build() -> None:
     ref_root = os.environ.get("EVX_REFERENCE_ROOT", "/root/reference")
     if os.path.isdir(os.path.join(ref_root, "plugins")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
+    if os.path.isdir(os.path.join(ref_root, "system", "tmine")):
+        # the reference's generated search for each constrained bench query
+        from oracle import ref_generated
+        ref_generated.build_bench_queries()
 
 
 def lib():

@@ -1,14 +1,12 @@
 """Write constraint_golden.json: constrained counts computed by the
 reference's OWN generated search code, checked against the oracle.
 
-For every case the reference's KernelGen (system/tmine/KernelGen.py, run
-from a scratch copy of the reference's system/ tree, since it writes the
-constraint snippets into its template directory: Query.py:135-160) renders
-the per-query CUDA search with warpCentric, warpBalancing and tailExpansion
-off, so one CUDA thread runs one root's sequential search.  The kernel body
-(everything before the host launcher) is compiled for the host with
-gen_shim.h and run over every root by gen_driver.cc.  The oracle
-(oracle/evx_oracle_cons.c) must agree on every case, or nothing is written.
+For every case the reference's KernelGen renders the per-query CUDA search
+with warpCentric, warpBalancing and tailExpansion off, so one CUDA thread runs
+one root's sequential search; oracle/ref_generated.py compiles that kernel
+body for the host (oracle/gen_shim.h, oracle/gen_driver.cc) and runs it over
+every root.  The oracle (oracle/evx_oracle_cons.c) must agree on every case,
+or nothing is written.
 
 Needs the reference tree (EVX_REFERENCE_ROOT, default /root/reference),
 g++ and PyYAML; run it where those exist:
@@ -17,14 +15,10 @@ g++ and PyYAML; run it where those exist:
 """
 from __future__ import annotations
 
-import ctypes
 import json
 import os
-import shutil
-import subprocess
 import sys
 import tempfile
-import types
 
 import numpy as np
 
@@ -34,8 +28,8 @@ sys.path.insert(0, ROOT)
 
 from everest_b200.constraints import Constraints  # noqa: E402
 from oracle import oracle as O  # noqa: E402
+from oracle import ref_generated as RG  # noqa: E402
 
-REF = os.environ.get("EVX_REFERENCE_ROOT", "/root/reference")
 GRAPHS = {"tiny-ties": 2, "dense-4": 20, "mid-ties": 5, "mid-uniform": 250, "mid-hub": 1000,
           "zipf-2k-10k": 200000}
 MOTIFS = {
@@ -90,56 +84,9 @@ def constraint_sets(name, k, n, delta):
     return out
 
 
-def load_kernelgen(scratch):
-    shutil.copytree(os.path.join(REF, "system"), os.path.join(scratch, "system"))
-    pkg = types.ModuleType("tmine")
-    pkg.__path__ = [os.path.join(scratch, "system", "tmine")]
-    sys.modules["tmine"] = pkg  # bypass tmine/__init__ (it imports the compiled corelib)
-    from tmine import KernelGen as KG, Query as Q  # noqa: E402
-    return KG, Q
-
-
-def render(KG, Q, scratch, mu, mv, cons, enum_cap=0):
-    motif = os.path.join(scratch, "motif.txt")
-    with open(motif, "w") as f:
-        for i, (a, b) in enumerate(zip(mu, mv)):
-            f.write(f"{a + 1} {b + 1} {i + 1}\n")
-    q = Q.Query.__new__(Q.Query)
-    opts = {"gpu": 1, "warpCentric": False, "warpBalancing": False, "tailExpansion": False}
-    if enum_cap:
-        opts["enumerate"] = enum_cap
-    q.queryFile = {"pattern": motif, "graph": "-", "constraints": cons, "options": opts}
-    q.name = "fixture"
-    q.cons = Q.Constraints(cons)
-    opts = Q.Options()
-    opts.update(Q.Options(q.queryFile["options"]))
-    q.opts = opts
-    q.cons.genConsTemplates()
-    src = KG.KernelGen(motif, q).generate()
-    body = []
-    for line in src.split("\n"):
-        if line.startswith("// -----"):
-            break
-        if line.lstrip().startswith("#include"):
-            continue
-        body.append(line)
-    return "\n".join(body) + "\n"
-
-
-def build_lib(scratch, body, tag, enum=False):
-    inc = os.path.join(scratch, f"body_{tag}.inc")
-    with open(inc, "w") as f:
-        f.write(body)
+def build(scratch, mu, mv, cons, tag, enum_cap=0):
     so = os.path.join(scratch, f"gen_{tag}.so")
-    subprocess.run(["g++", "-O1", "-std=c++17", "-fPIC", "-shared", "-w", "-fpermissive", f"-I{HERE}",
-                    f'-DGEN_BODY="{inc}"'] + (["-DGEN_ENUM"] if enum else []) +
-                   ["-o", so, os.path.join(HERE, "gen_driver.cc")], check=True)
-    L = ctypes.CDLL(so)
-    ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
-    L.gen_count.argtypes = [ip, ctypes.c_int, ip, ip, ip, ip, ip, ip, ip, ip, ctypes.c_int,
-                            ctypes.c_int, ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_ulonglong)]
-    L.gen_count.restype = ctypes.c_int
-    return L
+    return RG.GeneratedSearch(RG.compile_body(RG.render(mu, mv, cons, enum_cap), so, enum=enum_cap > 0))
 
 
 def main():
@@ -148,26 +95,17 @@ def main():
     feats = {}
     cases = []
     with tempfile.TemporaryDirectory() as scratch:
-        KG, Q = load_kernelgen(scratch)
         tag = 0
         for gname, delta in GRAPHS.items():
             g = O.Graph(d[gname + "_u"], d[gname + "_v"], d[gname + "_t"], int(d[gname + "_V"][0]))
             nf = rng.integers(0, 10, g.V).astype(np.int32)
             ef = rng.integers(0, 10, max(g.E, 1)).astype(np.int32)
             feats[gname + "_node"], feats[gname + "_edge"] = nf, ef
-            eg = np.stack([g.u, g.v, g.t], axis=1).astype(np.int32).ravel()
             for mname, (mu, mv) in MOTIFS.items():
                 k, n = len(mu), max(max(mu), max(mv)) + 1
                 for cons in constraint_sets(mname, k, n, delta):
-                    body = render(KG, Q, scratch, mu, mv, cons)
-                    L = build_lib(scratch, body, tag)
+                    ref = build(scratch, mu, mv, cons, tag).run(g, nf, ef, mu, mv, delta)
                     tag += 1
-                    work = max(0, g.E - k + 1)
-                    out = ctypes.c_ulonglong(0)
-                    L.gen_count(eg, g.E, g.in_eid, g.in_off, g.out_eid, g.out_off, nf, ef,
-                                np.asarray(mu, np.int32), np.asarray(mv, np.int32), k, delta, work,
-                                np.zeros(1, np.int32), np.zeros(1, np.int32), ctypes.byref(out))
-                    ref = int(out.value)
                     c = Constraints.from_yaml(cons, mu, mv).to_struct()
                     mine = O.count_constrained(g, mu, mv, delta, c, nf, ef)
                     if mine != ref:
@@ -184,15 +122,9 @@ def main():
             mu, mv = MOTIFS[mname]
             k = len(mu)
             cons = dict(cons, delta=GRAPHS[gname])
-            L = build_lib(scratch, render(KG, Q, scratch, mu, mv, cons, ENUM_CAP), tag, enum=True)
-            tag += 1
-            eg = np.stack([g.u, g.v, g.t], axis=1).astype(np.int32).ravel()
             rows = np.zeros(ENUM_CAP * k, np.int32)
-            out = ctypes.c_ulonglong(0)
-            L.gen_count(eg, g.E, g.in_eid, g.in_off, g.out_eid, g.out_off, nf, ef, np.asarray(mu, np.int32),
-                        np.asarray(mv, np.int32), k, GRAPHS[gname], max(0, g.E - k + 1), rows,
-                        np.arange(max(g.E, 1), dtype=np.int32), ctypes.byref(out))
-            total = int(out.value)
+            total = build(scratch, mu, mv, cons, tag, ENUM_CAP).run(g, nf, ef, mu, mv, GRAPHS[gname], rows)
+            tag += 1
             if not 0 < total < ENUM_CAP:
                 raise SystemExit(f"enumeration case {gname} {mname} {cons}: total {total}")
             ref_rows = sorted(map(tuple, rows[: total * k].reshape(total, k).tolist()))
@@ -203,6 +135,7 @@ def main():
             enum_cases.append({"graph": gname, "motif": mname, "mu": mu, "mv": mv, "delta": GRAPHS[gname],
                                "constraints": cons, "total": total, "rows": [list(r) for r in ref_rows]})
             print(f"enumerate {gname:12s} {mname:8s} {total:6d} rows")
+    RG.cleanup()
     np.savez_compressed(os.path.join(HERE, "constraint_features.npz"), **feats)
     with open(os.path.join(HERE, "constraint_golden.json"), "w") as f:
         json.dump({"source": "reference KernelGen output (warp options off) run on the host; "
