@@ -101,6 +101,7 @@ typedef struct {
 
 typedef struct {
   uint64_t count;
+  uint64_t roots, r_reads, candidates;  /* the algorithmic-bytes counters of evx_oracle.c */
   int m[EVX_MAX_MOTIF_NODES + 1];
   int e[EVX_MAX_MOTIF_EDGES];
   int *rows;
@@ -157,18 +158,22 @@ static void cdfs(const cons_ctx *x, cons_state *s, int j) {
     const int ma = s->m[a], mb = s->m[b];
     const int ib = x->in_off[mb], ie = x->in_off[mb + 1];
     const int ob = x->out_off[ma], oe = x->out_off[ma + 1];
+    s->r_reads += 2;
     if (ie - ib < oe - ob) { lst = x->in_eid; lo = ib; hi = ie; want = ma; other_is_v = 0; }
     else { lst = x->out_eid; lo = ob; hi = oe; want = mb; other_is_v = 1; }
   } else if (b >= nm) {
     lst = x->out_eid; lo = x->out_off[s->m[a]]; hi = x->out_off[s->m[a] + 1]; other_is_v = 1;
+    s->r_reads += 1;
   } else {
     lst = x->in_eid; lo = x->in_off[s->m[b]]; hi = x->in_off[s->m[b] + 1]; other_is_v = 0;
+    s->r_reads += 1;
   }
   lo = first_after(lst, lo, hi, pr);
   const int anti = (c->anti_mask >> j) & 1;
   const int last = (j == x->k - 1);
   for (int p = lo; p < hi; p++) {
     const int ce = lst[p];
+    s->candidates++;
     if (x->t[ce] > tl) break;
     const int node = other_is_v ? x->v[ce] : x->u[ce];
     int ok;
@@ -203,6 +208,7 @@ static void cdfs(const cons_ctx *x, cons_state *s, int j) {
 }
 
 static void cons_root(const cons_ctx *x, cons_state *s, int64_t r) {
+  s->roots++;
   if (x->u[r] == x->v[r]) return;
   if (!node_ok(x, x->u[r], 0) || !node_ok(x, x->v[r], 1) || !edge_ok(x, (int)r)) return;
   s->m[0] = x->u[r];
@@ -235,31 +241,40 @@ static int cons_setup(cons_ctx *x, const int *u, const int *v, const int *t,
   return 0;
 }
 
-/* Constrained count over roots [root_beg, root_end). */
+/* Constrained count over roots [root_beg, root_end).  stats (may be NULL)
+ * receives {roots, r_reads, candidates} as evx_oracle.c counts them. */
 int oracle_count_constrained(const int *u, const int *v, const int *t,
                              const int *out_off, const int *out_eid,
                              const int *in_off, const int *in_eid,
                              const int *node_feat, const int *edge_feat,
                              int k, const int *mu, const int *mv, int delta,
                              const evx_constraints *c, int64_t root_beg, int64_t root_end,
-                             int nthreads, uint64_t *count_out) {
+                             int nthreads, uint64_t *count_out, uint64_t *stats) {
   cons_ctx x;
   if (cons_setup(&x, u, v, t, out_off, out_eid, in_off, in_eid, node_feat, edge_feat, k, mu, mv,
                  delta, c))
     return -1;
-  uint64_t total = 0;
+  uint64_t total = 0, roots = 0, rr = 0, cand = 0;
 #ifdef _OPENMP
   if (nthreads <= 0) nthreads = omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads) reduction(+ : total)
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads) reduction(+ : total, roots, rr, cand)
 #endif
   for (int64_t r = root_beg; r < root_end; r++) {
     cons_state s;
     memset(&s, 0, sizeof(s));
     cons_root(&x, &s, r);
     total += s.count;
+    roots += s.roots;
+    rr += s.r_reads;
+    cand += s.candidates;
   }
   (void)nthreads;
   *count_out = total;
+  if (stats) {
+    stats[0] = roots;
+    stats[1] = rr;
+    stats[2] = cand;
+  }
   return 0;
 }
 

@@ -318,7 +318,8 @@ def _cons_lib():
     if not getattr(L, "_cons_ready", False):
         args = [_i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, ctypes.c_void_p, ctypes.c_void_p,
                 ctypes.c_int, _i32p, _i32p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64]
-        L.oracle_count_constrained.argtypes = args + [ctypes.c_int, ctypes.POINTER(ctypes.c_uint64)]
+        L.oracle_count_constrained.argtypes = args + [ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
+                                                      ctypes.c_void_p]
         L.oracle_count_constrained.restype = ctypes.c_int
         L.oracle_enumerate_constrained.argtypes = args + [ctypes.c_void_p, ctypes.c_int64,
                                                           ctypes.POINTER(ctypes.c_uint64)]
@@ -337,18 +338,23 @@ def _feat_ptr(a):
 
 
 def count_constrained(g: Graph, mu, mv, delta: int, cons, node_feat=None, edge_feat=None,
-                      roots=None, threads: int = 0) -> int:
-    """Constrained count; cons is an everest_b200.constraints.EvxConstraints."""
+                      roots=None, threads: int = 0, stats: Optional[dict] = None) -> int:
+    """Constrained count; cons is an everest_b200.constraints.EvxConstraints.
+    stats, when given, receives roots / r_reads / candidates (the
+    algorithmic-bytes counters of the plain oracle)."""
     k = len(mu)
     rb, re_ = roots if roots is not None else default_roots(g, k)
     a_mu, a_mv = _motif_arrays(mu, mv)
     nf, ef = _feat_ptr(node_feat), _feat_ptr(edge_feat)
     out = ctypes.c_uint64(0)
+    st = (ctypes.c_uint64 * 3)()
     rc = _cons_lib().oracle_count_constrained(
         *g._args(), nf[1] if nf else None, ef[1] if ef else None, k, a_mu, a_mv, int(delta),
-        ctypes.addressof(cons), int(rb), int(re_), int(threads), ctypes.byref(out))
+        ctypes.addressof(cons), int(rb), int(re_), int(threads), ctypes.byref(out), ctypes.addressof(st))
     if rc != 0:
         raise ValueError("motif or constraints violate the search precondition")
+    if stats is not None:
+        stats.update(roots=int(st[0]), r_reads=int(st[1]), candidates=int(st[2]))
     return int(out.value)
 
 
