@@ -25,7 +25,7 @@ import ctypes
 import itertools
 import os
 import subprocess
-from typing import List, Optional, Sequence, Tuple
+from typing import List, Optional, Tuple
 
 import numpy as np
 
