@@ -60,6 +60,17 @@ class ConstraintError(ValueError):
     pass
 
 
+def _flag(x) -> bool:
+    """An antiEdge entry as the reference renders it into C++
+    (str(x).lower(), Query.py:44-50): true / false, or 1 / 0."""
+    text = str(x).strip().lower()
+    if text in ("true", "1"):
+        return True
+    if text in ("false", "0"):
+        return False
+    raise ConstraintError(f"antiEdge entry {x!r} is not a boolean")
+
+
 class Constraints:
     """Validated, compiled constraints of one query on one motif."""
 
@@ -97,7 +108,7 @@ class Constraints:
             raise ConstraintError(f"unsupported constraint {key!r}")
         # anti-edges
         if "antiEdge" in cons:
-            anti = [bool(x) for x in cons["antiEdge"]]
+            anti = [_flag(x) for x in cons["antiEdge"]]
             if len(anti) != k:
                 raise ConstraintError(f"antiEdge has {len(anti)} entries for a {k}-edge motif")
             for j in (0, 1, k - 1):

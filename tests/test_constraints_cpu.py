@@ -154,6 +154,11 @@ def test_constraint_checks():
     for cons, msg in bad:
         with pytest.raises((ConstraintError, consexpr.ExprError), match=msg):
             Constraints.from_yaml(dict(cons, delta=3600), *m4a)
+    # entries as the reference renders them into C++: true / false / 1 / 0, any case
+    st = Constraints.from_yaml({"delta": 1, "antiEdge": ["False", 0, "TRUE", False, "false"]}, *m4a).to_struct()
+    assert st.anti_mask == 4
+    with pytest.raises(ConstraintError, match="not a boolean"):
+        Constraints.from_yaml({"delta": 1, "antiEdge": [False, False, "yes", False, False]}, *m4a)
     # an anti-edge must join nodes that earlier real edges map
     with pytest.raises(ConstraintError, match="no earlier real edge"):
         Constraints.from_yaml({"delta": 1, "antiEdge": [False, False, True, False]},
