@@ -13,7 +13,9 @@ Accepted keys (besides `delta`):
   edge                    one predicate in `f` for every edge
   temporal                k-1 gap bounds (extra ones are ignored)
   antiEdge                k booleans
-  filter                  an expression in e0 .. e{k-1}
+  filter                  an expression in e0 .. e{k-1} (the reference's
+                          generated code declares eid0 .. eid{k-2} only, so
+                          naming the last edge, e{k-1}, is an extension)
 
 Refused, with the reason:
   edge0, edge1, ...       the reference applies edge1's predicate to e_0 and
