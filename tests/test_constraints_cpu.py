@@ -1,6 +1,7 @@
 """Constraint features on the CPU: the expression compiler against C's own
 arithmetic, the oracle against the reference's generated code (fixtures),
 and the checks that refuse what the reference cannot run."""
+import ctypes
 import json
 import os
 import random
@@ -275,3 +276,26 @@ def test_oracle_matches_brute_force_semantics():
         assert got == want, (trial, cons, got, want)
         checked += want > 0
     assert checked > 40
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")
+def test_struct_layout_matches_the_c_header():
+    """The ctypes mirror of evx_constraints / evx_program has the C layout."""
+    from everest_b200.constraints import EvxConstraints
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    fields = ["anti_mask", "has_temporal", "temporal", "node_mode", "node", "has_edge", "edge", "has_filter",
+              "filter"]
+    src = ["#include <stdio.h>", "#include <stddef.h>", '#include "everest_b200.h"', "int main(void) {",
+           '  printf("%zu %zu\\n", sizeof(evx_constraints), sizeof(evx_program));']
+    src += [f'  printf("%zu\\n", offsetof(evx_constraints, {f}));' for f in fields]
+    src += ["  return 0; }"]
+    with tempfile.TemporaryDirectory() as tmp:
+        c = os.path.join(tmp, "x.c")
+        with open(c, "w") as f:
+            f.write("\n".join(src))
+        exe = os.path.join(tmp, "x")
+        subprocess.run(["gcc", "-I", os.path.join(root, "include"), "-o", exe, c], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
+    assert int(out[0]) == ctypes.sizeof(EvxConstraints) and int(out[1]) == ctypes.sizeof(EvxProgram)
+    for f, off in zip(fields, out[2:]):
+        assert getattr(EvxConstraints, f).offset == int(off), f
