@@ -31,6 +31,19 @@ std::vector<int> take_ints(int *p, size_t n) {
   return v;
 }
 
+// The first min(n, file length) int32 values of a raw file (a random-feature
+// file can be far longer than the graph needs: read only the prefix).
+bool read_ints_prefix(const std::filesystem::path &p, size_t n, std::vector<int> &out) {
+  std::ifstream f(p, std::ios::binary | std::ios::ate);
+  if (!f) return false;
+  const std::streamsize sz = f.tellg();
+  if (sz < 0) return false;
+  const size_t have = (size_t)sz / 4;
+  out.resize(std::min(n, have));
+  f.seekg(0);
+  return (bool)f.read(reinterpret_cast<char *>(out.data()), (std::streamsize)(out.size() * 4));
+}
+
 bool read_ints(const std::filesystem::path &p, std::vector<int> &out) {
   std::ifstream f(p, std::ios::binary | std::ios::ate);
   if (!f) return false;
@@ -106,15 +119,16 @@ FeatureLoader::FeatureLoader(const EdgeListLoader *eloader, const std::filesyste
     vertexIds_ = std::move(fvm);
     return;
   }
-  std::vector<int> r;
-  if (pathToRands.empty() || !read_ints(pathToRands, r)) return;
-  if (r.size() >= E) edge_.assign(r.begin(), r.begin() + (long)E);
+  if (pathToRands.empty()) return;
   // distinct vertex ids, ascending; vertex i of that order takes value i
   // (src/core/gpu/data.cu:57-79)
   std::vector<int> ids(eloader->U());
   ids.insert(ids.end(), eloader->V().begin(), eloader->V().end());
   std::sort(ids.begin(), ids.end());
   ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+  std::vector<int> r;
+  if (!read_ints_prefix(pathToRands, std::max(E, ids.size()), r)) return;
+  if (r.size() >= E) edge_.assign(r.begin(), r.begin() + (long)E);
   if (r.size() >= ids.size()) {
     vertex_.assign(r.begin(), r.begin() + (long)ids.size());
     vertexIds_ = std::move(ids);
