@@ -417,7 +417,7 @@ def main():
     if args.single_query >= 0:
         return run_single_query(args)
     if args.mode in ("batch", "serve", "enumerate", "constrained"):
-        from everest_b200 import bench_modes
+        import bench_modes
         return bench_modes.run(args)
     if args.impl == "reference":
         return run_reference_arm(args)

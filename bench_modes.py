@@ -71,7 +71,7 @@ def _pct(x, p):
 
 def run_batch(args) -> int:
     import torch
-    from . import autotune, capi, synth, workloads
+    from everest_b200 import autotune, capi, synth, workloads
     torch.cuda.set_device(0)
     window = args.window or 1_000_000
     n = args.queries or 64
@@ -133,7 +133,7 @@ def run_batch(args) -> int:
 
 def run_serve(args) -> int:
     import torch
-    from . import capi, serve, synth, workloads
+    from everest_b200 import capi, serve, synth, workloads
     torch.cuda.set_device(0)
     window = args.window or 100_000
     n = args.queries or 2000
@@ -238,7 +238,7 @@ def run_enumerate(args) -> int:
     its time, and a host check that every returned row is a distinct valid
     match (edge order, window, endpoints, injectivity)."""
     import torch
-    from . import capi, synth
+    from everest_b200 import capi, synth
     torch.cuda.set_device(0)
     spec = synth.SPECS["bursty-2.6m-36m"]
     u, v, t = synth.load_or_generate(spec.name)
@@ -294,7 +294,7 @@ def constrained_cpu(u, v, t, queries, nf, ef) -> List[dict]:
     build had the reference tree) and through the oracle."""
     from oracle import oracle as O
     from oracle import ref_generated as RG
-    from .constraints import Constraints
+    from everest_b200.constraints import Constraints
     V = int(max(u.max(), v.max())) + 1
     g = O.Graph(u, v, t, V)
     out = []
@@ -322,8 +322,8 @@ def run_constrained(args) -> int:
     generated search built for the host (where present) and the oracle, with
     their times on all host cores; the reference's is the cpu_baseline."""
     import torch
-    from . import capi, synth, workloads
-    from .constraints import Constraints
+    from everest_b200 import capi, synth, workloads
+    from everest_b200.constraints import Constraints
     torch.cuda.set_device(0)
     spec = synth.SPECS["bursty-1.1m-7.8m"]
     u, v, t = synth.load_or_generate(spec.name)

@@ -35,6 +35,8 @@
 //  * enumeration slots are reserved with one warp-aggregated atomicAdd per
 //    step (the reference issues one atomicAdd per match,
 //    system/tmine/KernelGen.py:505-524).
+#include <atomic>
+
 #include "evx_internal.cuh"
 
 namespace evx {
@@ -977,20 +979,25 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
   flush();
 }
 
+// The shared-memory attribute belongs to the function on the current
+// device, so it is set once per device (bit d of the mask: device d).
 template <int K, bool ENUM, bool EXACT>
 int setup_k() {
-  static bool done = false;  // per process; the attribute is per function
-  if (!done) {
-    cudaError_t e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)(kWarps * sizeof(WarpSmem<K>)));
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  static std::atomic<unsigned long long> done{0ull};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return 0;
+  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(kWarps * sizeof(WarpSmem<K>)));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
 #ifdef EVX_CARVEOUT
-    e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             EVX_CARVEOUT);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(carveout)");
+  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           EVX_CARVEOUT);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(carveout)");
 #endif
-    done = true;
-  }
+  done.fetch_or(bit, std::memory_order_release);
   return 0;
 }
 

@@ -50,11 +50,23 @@ class OracleStats(ctypes.Structure):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
 
+def reference_root() -> Optional[str]:
+    """The reference checkout named by EVX_REFERENCE_ROOT, or None when the
+    variable is unset or does not name one (the builds that read it are then
+    skipped; their outputs under oracle/_ref/ run without it)."""
+    r = os.environ.get("EVX_REFERENCE_ROOT")
+    if r and os.path.isdir(os.path.join(r, "plugins")) and os.path.isdir(os.path.join(r, "system", "tmine")):
+        return r
+    return None
+
+
 def build() -> None:
-    """Compile the oracle (and, where the reference tree exists, the host
-    build of the reference's Baseline body)."""
+    """Compile the oracle (and, where EVX_REFERENCE_ROOT names the reference
+    tree, the host build of the reference's Baseline body)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    ref_root = os.environ.get("EVX_REFERENCE_ROOT", "/root/reference")
+    ref_root = reference_root()
+    if ref_root is None:
+        return
     if os.path.isdir(os.path.join(ref_root, "plugins")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
     if os.path.isdir(os.path.join(ref_root, "system", "tmine")):

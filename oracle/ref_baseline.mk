@@ -5,7 +5,10 @@
 # become host functions, a loop over root ids replaces the CUDA grid, and
 # atomicAdd becomes a relaxed atomic add.  Nothing is copied into the
 # repository: the extracted lines go to $(OUT) (git-ignored) only.
-REF ?= /root/reference
+REF ?= $(EVX_REFERENCE_ROOT)
+ifeq ($(strip $(REF)),)
+$(error set EVX_REFERENCE_ROOT (or REF=) to the reference checkout)
+endif
 HERE := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
 OUT ?= $(HERE)_ref
 SRC := $(REF)/plugins/GPUWorkerBaseline.cu

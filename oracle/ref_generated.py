@@ -13,8 +13,8 @@ warpBalancing and tailExpansion off each CUDA thread runs one root's
 sequential search; that kernel body (everything before the host launcher)
 is compiled for the host with gen_shim.h and run over every root by
 gen_driver.cc, one OpenMP iteration per root.  Rendering needs the
-reference tree (EVX_REFERENCE_ROOT, default /root/reference); the built
-libraries under oracle/_ref/ run without it.
+reference tree, named by EVX_REFERENCE_ROOT; the built libraries under
+oracle/_ref/ run without it.
 """
 from __future__ import annotations
 
@@ -31,13 +31,17 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
-REF_ROOT = os.environ.get("EVX_REFERENCE_ROOT", "/root/reference")
 
 _kg = None
 
 
+def reference_root() -> Optional[str]:
+    r = os.environ.get("EVX_REFERENCE_ROOT")
+    return r if r and os.path.isdir(os.path.join(r, "system", "tmine")) else None
+
+
 def available() -> bool:
-    return os.path.isdir(os.path.join(REF_ROOT, "system", "tmine"))
+    return reference_root() is not None
 
 
 def _kernelgen():
@@ -45,7 +49,10 @@ def _kernelgen():
     global _kg
     if _kg is None:
         scratch = tempfile.mkdtemp(prefix="evx-kernelgen-")
-        shutil.copytree(os.path.join(REF_ROOT, "system"), os.path.join(scratch, "system"))
+        ref = reference_root()
+        if ref is None:
+            raise RuntimeError("set EVX_REFERENCE_ROOT to a reference checkout")
+        shutil.copytree(os.path.join(ref, "system"), os.path.join(scratch, "system"))
         pkg = types.ModuleType("tmine")
         pkg.__path__ = [os.path.join(scratch, "system", "tmine")]
         sys.modules["tmine"] = pkg  # bypass tmine/__init__ (it imports the compiled corelib)

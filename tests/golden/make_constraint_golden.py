@@ -8,7 +8,7 @@ body for the host (oracle/gen_shim.h, oracle/gen_driver.cc) and runs it over
 every root.  The oracle (oracle/evx_oracle_cons.c) must agree on every case,
 or nothing is written.
 
-Needs the reference tree (EVX_REFERENCE_ROOT, default /root/reference),
+Needs the reference tree (named by EVX_REFERENCE_ROOT),
 g++ and PyYAML; run it where those exist:
 
     python tests/golden/make_constraint_golden.py

@@ -28,7 +28,7 @@ sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 from everest_b200 import synth  # noqa: E402
 
-REF = os.environ.get("EVX_REFERENCE_ROOT", "/root/reference")
+REF = O.reference_root()  # EVX_REFERENCE_ROOT; required (the script refuses to run without it)
 
 
 def graph_digest(u, v, t) -> str:
@@ -166,4 +166,6 @@ def main():
 
 
 if __name__ == "__main__":
+    if REF is None:
+        raise SystemExit("set EVX_REFERENCE_ROOT to the reference checkout")
     main()

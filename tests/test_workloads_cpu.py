@@ -2,7 +2,8 @@
 two arms are compared by (CPU only)."""
 import numpy as np
 
-from everest_b200 import bench_modes, synth, workloads
+import bench_modes
+from everest_b200 import synth, workloads
 
 
 def test_batch_and_serve_mixes_are_seeded_and_in_range():
