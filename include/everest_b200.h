@@ -243,7 +243,10 @@ EVX_API int evx_batch_set_limit(evx_batch *b, uint64_t max_work);
  * delta[q]; roots are [beg, end) (end < 0: E - k + 1).  The first call on a
  * device looks up the array's device address, so it must come before any
  * stream capture.  All calls share the array: calls whose GPU work overlaps
- * race, so serialise them.  Rejects nq > EVX_STATIC_MAX_QUERIES. */
+ * race, so serialise them.  Rejects nq > EVX_STATIC_MAX_QUERIES.  Every
+ * query is checked before the first launch (an error for a bad query leaves
+ * nothing queued); the call returns once the counts are in host memory (it
+ * waits for `stream`), and it leaves the caller's current device as it was. */
 #define EVX_STATIC_MAX_QUERIES 256
 EVX_API int evx_count_static(const evx_graph *g, int nq, const int *k, const int *mu,
                              const int *mv, const int *delta, int64_t beg, int64_t end,

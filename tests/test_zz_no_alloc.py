@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 from everest_b200 import capi, synth
+from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -28,29 +29,64 @@ QUERIES = [
 ]
 
 
+SPEC = synth.GraphSpec("static-zipf", "zipf", 800, 30_000, seed=17, t_max=300_000)
+
+
 @pytest.fixture(scope="module")
-def graph():
-    spec = synth.GraphSpec("static-zipf", "zipf", 800, 30_000, seed=17, t_max=300_000)
-    u, v, t = synth.generate(spec)
+def edges():
+    return synth.generate(SPEC)
+
+
+@pytest.fixture(scope="module")
+def graph(edges):
+    u, v, t = edges
     dg = capi.DeviceGraph(capi.graph_build_host(u, v, t), 0)
     yield dg
     dg.free()
 
 
-def test_static_count_equals_worker_twice(graph):
+def _worker_counts(graph, beg=0, end=-1):
     w = capi.Worker(0)
     want = []
     for mu, mv, d in QUERIES:
-        w.take(graph, mu, mv, d)
+        w.take(graph, mu, mv, d, beg, end)
         want.append(w.run())
     w.close()
+    return want
+
+
+def test_static_count_equals_worker_and_oracle_twice(graph, edges):
+    want = _worker_counts(graph)
     assert sum(want) > 0
+    g = O.Graph(*edges, SPEC.num_nodes)
+    assert want == [O.count(g, mu, mv, d)[0] for mu, mv, d in QUERIES]
     first = capi.count_static(graph, QUERIES)
     second = capi.count_static(graph, QUERIES)  # the array keeps the last call's contents
     assert first == want
     assert second == want
     # a single query reusing slot 0 after a larger call
     assert capi.count_static(graph, QUERIES[3:4]) == want[3:4]
+
+
+def test_static_count_root_window_on_a_worker_stream(graph, edges):
+    beg, end = 4_000, 21_000
+    want = _worker_counts(graph, beg, end)
+    g = O.Graph(*edges, SPEC.num_nodes)
+    assert want == [O.count(g, mu, mv, d, roots=(beg, end))[0] for mu, mv, d in QUERIES]
+    side = capi.Worker(0)  # owns a non-default stream
+    try:
+        for _ in range(2):
+            assert capi.count_static(graph, QUERIES, beg, end, stream=side.stream) == want
+    finally:
+        side.close()
+
+
+def test_static_count_bad_last_query_launches_nothing(graph):
+    want = _worker_counts(graph)
+    bad = QUERIES + [([0, 1, 2], [1, 2, 0], -5)]  # negative delta: rejected
+    with pytest.raises(capi.EvxError):
+        capi.count_static(graph, bad)
+    assert capi.count_static(graph, QUERIES) == want
 
 
 def test_static_count_rejects_too_many_queries(graph):
