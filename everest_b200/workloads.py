@@ -77,6 +77,19 @@ def batch_queries(window: int = 1_000_000, n: int = 64) -> List[dict]:
                          deltas=(3600, 86400, 604800))
 
 
+# The 16 queries of the 64-query mix whose search over the whole 36M-edge
+# graph is cheapest (1.6-6 ms each for this library on a B200; of the other
+# 48, 29 examine more than 3e9 adjacency records each).
+BATCH_SLICE = (36, 63, 30, 3, 10, 48, 19, 0, 6, 1, 24, 39, 51, 49, 57, 15)
+
+
+def refgen_batch_slice() -> List[dict]:
+    """BATCH_SLICE of the 64-query batch mix over every root of the graph:
+    the full-size slice the reference's generated kernel checks."""
+    qs = batch_queries()
+    return [dict(qs[i], name=f"batch-{i:02d}", beg=0, end=-1) for i in BATCH_SLICE]
+
+
 def serve_queries(window: int = 100_000, n: int = 10_000) -> List[dict]:
     """Serving stream: 3-5-edge patterns on 2-4 nodes over the 7.8M- and
     63M-edge graphs, delta log-uniform in [600, 604800], 20% enumerations
