@@ -10,9 +10,11 @@ sample, which is checked) and caches the winner per key:
     key = (graph fingerprint, motif edges, floor(log2(delta + 1)))
 
 Knobs: resident blocks per SM (0 = occupancy), intra-warp rebalance interval
-and minimum split width ("steal granularity"), and how the last edge is
+and minimum split width ("steal granularity"), how the last edge is
 counted: range arithmetic on the pair index, a pair hash-table or
-pair-directory lookup per partial match, or a scan ("tail-expansion depth").  Batches are tuned on
+pair-directory lookup per partial match, or a scan ("tail-expansion depth"),
+and whether an edge between two mapped nodes walks its pair run or scans the
+shorter adjacency list.  Batches are tuned on
 their tile size.
 """
 from __future__ import annotations
@@ -39,6 +41,7 @@ CANDIDATES = [
     {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_NO_CLOSING_PRUNE},
     {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_NEW_SCAN},
     {"blocks_per_sm": 4, "steal_interval": 16, "min_split": 2, "flags": 0},
+    {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_LIST_SCAN},
 ]
 BATCH_TILES = (64, 128, 256, 512)
 

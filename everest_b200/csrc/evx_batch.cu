@@ -37,8 +37,8 @@ struct evx_batch {
   // tuning
   int tile_roots = 256, blocks_per_sm = 0, steal_interval = 16, min_split = 2, use_graph = 1;
   unsigned long long limit = 0;  // work limit per query (0 = none)
-  // table order -> query index, and the motif-size groups of the table:
-  // {k, first table position, queries, tiles, grid}
+  // table order -> query index, and the motif-size groups of the table
+  // (kGroupWords ints each)
   std::vector<int> order;
   std::vector<int> groups;
   // captured launch and the shape it was captured for
@@ -55,6 +55,9 @@ struct evx_batch {
 namespace {
 
 constexpr int kCursors = 8;  // one work-queue cursor word per motif size
+// a motif-size group of the table: {k, first table position, queries, tiles,
+// grid, pair-run walk (0/1)}
+constexpr int kGroupWords = 6;
 
 void drop_exec(evx_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -68,20 +71,21 @@ int enqueue(evx_batch *b, int nq) {
                            b->stream));
   EVX_CUDA(cudaMemsetAsync(b->counts_d, 0, sizeof(unsigned long long) * (2 * (size_t)b->max_q + kCursors),
                            b->stream));
-  for (size_t gi = 0; gi < b->groups.size(); gi += 5) {
+  for (size_t gi = 0; gi < b->groups.size(); gi += kGroupWords) {
     const int k = b->groups[gi], beg = b->groups[gi + 1], n = b->groups[gi + 2];
     const int tiles = b->groups[gi + 3], grid = b->groups[gi + 4];
+    const bool ps = b->groups[gi + 5] != 0;
     if (tiles <= 0) continue;
     LaunchArgs la;
     la.table = b->table_d + beg;
     la.nq = n;
     la.total_tiles = tiles;
     la.tile_roots = b->tile_roots;
-    la.cursor = reinterpret_cast<int *>(b->counts_d + b->max_q + gi / 5);
+    la.cursor = reinterpret_cast<int *>(b->counts_d + b->max_q + gi / kGroupWords);
     la.counts = b->counts_d + beg;
     la.limit = b->limit;
     la.meter = meter + beg;
-    int rc = launch_table(b->graph->g.view(), b->table_h[beg], la, k, grid, b->stream);
+    int rc = launch_table(b->graph->g.view(), b->table_h[beg], la, k, ps, grid, b->stream);
     if (rc) return rc;
     EVX_CUDA(cudaGetLastError());
   }
@@ -231,22 +235,25 @@ int evx_batch_launch(evx_batch *b) {
     const int k = b->queries[b->order[pos]].plan.k;
     const int beg = pos;
     int tiles = 0;
+    bool ps = false;
     for (; pos < nq && b->queries[b->order[pos]].plan.k == k; pos++) {
       QueryDesc q = b->queries[b->order[pos]];
+      ps = ps || plan_pair_scan(q.plan, q.flags, false);
       q.tile_beg = tiles;
       const int n = q.root_end - q.root_beg;
       tiles += n > 0 ? (n + b->tile_roots - 1) / b->tile_roots : 0;
       b->table_h[pos] = q;
     }
     int bps = 0;
-    int rc = table_occupancy(k, &bps);  // also sets the kernel attributes before any capture
+    int rc = table_occupancy(k, ps, &bps);  // also sets the kernel attributes before any capture
     if (rc) return rc;
     if (b->blocks_per_sm > 0) bps = b->blocks_per_sm;
     if (bps < 1) bps = 1;
-    b->groups.insert(b->groups.end(), {k, beg, pos - beg, tiles, bps * b->num_sms});
+    b->groups.insert(b->groups.end(), {k, beg, pos - beg, tiles, bps * b->num_sms, ps ? 1 : 0});
     launches += tiles > 0 ? 1 : 0;
   }
-  if ((int)b->groups.size() / 5 > kCursors) return fail(EVX_ERR_INVALID, "too many motif sizes in one batch");
+  if ((int)b->groups.size() / kGroupWords > kCursors)
+    return fail(EVX_ERR_INVALID, "too many motif sizes in one batch");
   EVX_CUDA(cudaEventRecord(b->ev0, b->stream));
   if (b->use_graph) {
     if (!b->exec || b->exec_nq != nq || b->exec_groups != b->groups || b->exec_tile_roots != b->tile_roots ||

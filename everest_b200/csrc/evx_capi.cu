@@ -108,7 +108,8 @@ int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
 // edge that maps a new node is scanned, and past the first step of a window
 // the rest is counted by range arithmetic (kQNewArith) unless asked not to.
 int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
-  const int np = (flags & EVX_FLAG_NO_CLOSING_PRUNE) ? kQNoPrune : 0;
+  const int np = ((flags & EVX_FLAG_NO_CLOSING_PRUNE) ? kQNoPrune : 0) |
+                 ((flags & (EVX_FLAG_LIST_SCAN | EVX_FLAG_NO_PAIR_INDEX | EVX_FLAG_CLOSING_SCAN)) ? 0 : kQPairScan);
   const int k = plan.k;
   if (enumerate || (flags & EVX_FLAG_NO_PAIR_INDEX) || k < 2) return np;
   const int wl = plan.info[k - 2];
@@ -667,7 +668,9 @@ int evx_worker_launch(evx_worker *w) {
   SearchArgs &a = w->args;
   int bps = w->blocks_per_sm;
   if (bps <= 0) {
-    int rc = search_occupancy(w->plan.k, a.enumerate != 0, w->block, &bps);
+    const int qf = (a.strict_ts ? kQStrict : 0) | a.tail_flags;
+    int rc = search_occupancy(w->plan.k, a.enumerate != 0, plan_pair_scan(w->plan, qf, a.enumerate != 0),
+                              w->block, &bps);
     if (rc) return rc;
     if (bps <= 0) bps = 1;
   }

@@ -118,6 +118,7 @@ constexpr int kQPairHash = 16;   // last edge's pair found through the pair hash
 constexpr int kQNoPrune = 32;    // no closing-endpoint check before a task's scan
 constexpr int kQRevPair = 64;    // last edge reverses the previous edge's endpoints
 constexpr int kQNewArith = 128;  // a new-node last edge's long windows counted by range arithmetic
+constexpr int kQPairScan = 256;  // a scanned edge between two mapped nodes walks its pair run
 struct QueryDesc {
   MotifPlan plan;
   int root_beg, root_end;  // root edge ids [beg, end)
@@ -236,11 +237,15 @@ int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &a
                   int grid, int block, cudaStream_t stream);
 // Launch a persistent search over a table of queries (count mode); q0 is
 // used when nq == 1.  Every query of the table has k edges.
-int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int k, int grid,
+int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int k, bool ps, int grid,
                  cudaStream_t stream);
-int table_occupancy(int k, int *blocks_per_sm);
-// Max resident blocks per SM for a given motif size / mode / block.
-int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm);
+int table_occupancy(int k, bool ps, int *blocks_per_sm);
+// Whether a query with these kQ flags walks a pair run at some level (the
+// kernels are compiled with and without that walk).
+bool plan_pair_scan(const MotifPlan &plan, int qflags, bool enumerate);
+// Max resident blocks per SM for a given motif size / mode / pair-run
+// variant / block.
+int search_occupancy(int k, bool enumerate, bool ps, int block, int *blocks_per_sm);
 
 // A constrained search (evx_constrained.cu).  prev_real[j] = the latest motif
 // edge before j that is not an anti-edge (0 for j = 1).

@@ -62,7 +62,10 @@ constexpr int kScanWide = EVX_SCAN_WIDE;
 #ifndef EVX_MINB3
 #define EVX_MINB3 8
 #endif
-constexpr int min_blocks(int k) { return k <= 3 ? EVX_MINB3 : (k == 4 ? 6 : 4); }
+#ifndef EVX_MINB4
+#define EVX_MINB4 6
+#endif
+constexpr int min_blocks(int k) { return k <= 3 ? EVX_MINB3 : (k == 4 ? EVX_MINB4 : 4); }
 
 template <int N>
 __device__ __forceinline__ int sel(const int (&a)[N], int i) {
@@ -235,7 +238,7 @@ struct Prev {
   int eid, t, src, dst, pop, pip;
 };
 
-template <int K, bool ENUM, bool EXACT>
+template <int K, bool ENUM, bool EXACT, bool PS>
 struct Searcher {
   static constexpr int L = K - 1;          // levels; level l opens motif edge l + 1
   static constexpr int N = K + 1;          // motif nodes <= k + 1
@@ -461,9 +464,32 @@ struct Searcher {
     const int nmc = plan_nm(w);
     int pos = 0, end = 0, want = -1, base = 0;
     bool out = true;
+    bool prun = false;  // the range is a run of pair_rec (the edge's static pair), not a list
     int blo = 0, bhi = 0;
     bool searching = false;
-    if (has) {
+    if (PS && has && kind == 2 && (qf & kQPairScan)) {
+      // both endpoints are mapped: walk the run of the static edge (ia, ib)
+      // after the previous edge; every entry matches structurally.  The run
+      // is located from the previous edge itself when it is that pair or its
+      // reverse, else by one hash probe (after the signature filter).
+      const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
+      prun = true; out = true; base = ia; want = ib;
+      int lo, hi;
+      if (ia == p.src && ib == p.dst) {
+        const int2 pl = __ldg(g.pair_loc + p.eid);
+        lo = pl.x + 1; hi = pl.y;
+        if (strict_()) lo = pair_first_t_after(g, lo, hi, p.t);
+      } else if (ia == p.dst && ib == p.src) {
+        const int2 rl = __ldg(g.rev_loc + p.eid);
+        lo = rl.x; hi = rl.y;
+        if (strict_()) lo = pair_first_t_after(g, lo, hi, p.t);
+      } else {
+        const int2 f = (EVX_PAIR_SIG == 0 || pair_maybe(g, ia, ib)) ? pair_find(g, ia, ib) : make_int2(0, 0);
+        hi = f.x + f.y;
+        lo = pair_first_key_after(g, f.x, hi, strict_() ? p.t : p.eid, strict_());
+      }
+      pos = lo; end = hi;
+    } else if (has) {
       const int ia = sel(m, plan_a(w)), ib = sel(m, plan_b(w));
       int lo, hi, sc;
       if (kind == 2) {
@@ -516,15 +542,23 @@ struct Searcher {
         const unsigned act = __ballot_sync(kFull, pos < end);
         if (!act) break;
         if (act != kFull && si && ((++steps) & (si - 1)) == 0)
-          rebalance(act, pos, end, want, out, base, slot, root, tl, m, e);
+          rebalance(act, pos, end, want, out, prun, base, slot, root, tl, m, e);
         bool emit = false;
         int last_eid = 0;
         if (pos < end) {
           const int4 *lst = out ? g.out_rec : g.in_rec;
           int4 rr[WIDE];
 #pragma unroll
-          for (int q = 0; q < WIDE; q++)
-            if (q == 0 || pos + q < end) rr[q] = __ldg(lst + pos + q);
+          for (int q = 0; q < WIDE; q++) {
+            if (q == 0 || pos + q < end) {
+              if (prun) {
+                const int2 pr = __ldg(g.pair_rec + pos + q);
+                rr[q] = make_int4(pr.x, want, pr.y, 0);
+              } else {
+                rr[q] = __ldg(lst + pos + q);
+              }
+            }
+          }
 #pragma unroll
           for (int q = 0; q < WIDE; q++) {
             if (pos < end) {
@@ -620,7 +654,7 @@ struct Searcher {
         if (cs >= cub) pos = end;
       }
       if (l == kr() - 3 && plan_kind(wl) == 2 && (la < nmc) != (lb < nmc) &&
-          !(qf & (kQInlineLast | kQNoPrune)) && has && pos < end) {
+          !(qf & (kQInlineLast | kQNoPrune)) && has && pos < end && !prun) {
         // the closing edge has one endpoint mapped before this level, fixed
         // for the task: when that node's list (out-list of a source, in-list
         // of a destination) has no entry after the previous edge inside the
@@ -687,12 +721,13 @@ struct Searcher {
             // park this level's state in shared memory while the warp descends,
             // so none of it stays live in registers across the nested batch
             sm.save[l][lane][0] = make_int4(pos, end, want, base);
-            sm.save[l][lane][1] = make_int4(slot, root, tl, (steps << 1) | (out ? 1 : 0));
+            sm.save[l][lane][1] = make_int4(slot, root, tl, (steps << 2) | (prun ? 2 : 0) | (out ? 1 : 0));
             __syncwarp();
             descend<l>();
             const int4 s0 = sm.save[l][lane][0], s1 = sm.save[l][lane][1];
             pos = s0.x; end = s0.y; want = s0.z; base = s0.w;
-            slot = s1.x; root = s1.y; tl = s1.z; out = (s1.w & 1) != 0; steps = s1.w >> 1;
+            slot = s1.x; root = s1.y; tl = s1.z; out = (s1.w & 1) != 0; prun = PS && (s1.w & 2) != 0;
+            steps = s1.w >> 2;
             if (sm.halt) pos = end;  // the query stopped: unwind this level too
             Prev dummy;
             int rr;
@@ -702,18 +737,38 @@ struct Searcher {
         }
         if (!act) break;
         if (act != kFull && si && ((++steps) & (si - 1)) == 0)
-          rebalance(act, pos, end, want, out, base, slot, root, tl, m, e);
+          rebalance(act, pos, end, want, out, prun, base, slot, root, tl, m, e);
         // the next kScanWide records of every lane's range in one round of
         // loads (one memory latency instead of kScanWide), then processed
         // one at a time; records not processed before a descend are
-        // loaded again after it
+        // loaded again after it.  A pair run's entries {eid, t} become
+        // out-list records of its source: {eid, target, t, position in
+        // in_rec}, with the position in out_rec beside them (pf).
         int4 rw[kScanWide];
+        int pf[kScanWide];
         {
           const int4 *lst = out ? g.out_rec : g.in_rec;
 #pragma unroll
           for (int q = 0; q < kScanWide; q++) {
             rw[q] = make_int4(0, 0, 0, 0);
-            if (pos + q < end) rw[q] = __ldg(lst + pos + q);
+            pf[q] = pos + q;
+            if (pos + q < end) {
+              if (prun) {
+                const int2 pr = __ldg(g.pair_rec + pos + q);
+                rw[q] = make_int4(pr.x, want, pr.y, 0);
+              } else {
+                rw[q] = __ldg(lst + pos + q);
+              }
+            }
+          }
+          if (prun && !inline_here) {
+#pragma unroll
+            for (int q = 0; q < kScanWide; q++) {
+              if (pos + q < end && rw[q].z <= tl) {
+                rw[q].w = __ldg(g.inpos + rw[q].x);
+                pf[q] = __ldg(&g.edges[rw[q].x].w) & kPosMask;
+              }
+            }
           }
         }
         if (inline_here) {
@@ -743,7 +798,7 @@ struct Searcher {
             int2 pl[kScanWide];
 #pragma unroll
             for (int q = 0; q < kScanWide; q++) {
-              if (!rev && rw[q].w >= 0) ok[q] = false;
+              if (!rev && !prun && rw[q].w >= 0) ok[q] = false;
               pl[q] = ok[q] ? __ldg((rev ? g.rev_loc : g.pair_loc) + rw[q].x) : make_int2(0, 0);
             }
 #pragma unroll
@@ -794,7 +849,7 @@ struct Searcher {
                 push = structural_ok(rc.y, want, nmc, m);
               }
             }
-            push_children<l>(push, slot, rc, out, base, pos - 1, root);
+            push_children<l>(push, slot, rc, out, base, pf[q], root);
             if (sm.nb[l + 1] >= 32) break;  // descend before the next push
           }
         }
@@ -805,8 +860,8 @@ struct Searcher {
   // Idle lanes take equal slices of the widest remaining range at this level.
   template <int NN, int EE>
   __device__ __forceinline__ void rebalance(unsigned act, int &pos, int &end, int &want, bool &out,
-                                            int &base, int &slot, int &root, int &tl, int (&m)[NN],
-                                            int (&e)[EE]) {
+                                            bool &prun, int &base, int &slot, int &root, int &tl,
+                                            int (&m)[NN], int (&e)[EE]) {
     const int width = end - pos;
     const unsigned wmax = __reduce_max_sync(kFull, (unsigned)(width > 0 ? width : 0));
     if ((int)wmax < sm.q.min_split) return;
@@ -831,14 +886,15 @@ struct Searcher {
       }
     }
     const int d_want = __shfl_sync(kFull, want, donor);
-    const int d_out = __shfl_sync(kFull, (int)out, donor);
+    const int d_out = __shfl_sync(kFull, (int)out | ((PS && prun) ? 2 : 0), donor);
     const int d_base = __shfl_sync(kFull, base, donor);
     const int d_slot = __shfl_sync(kFull, slot, donor);
     const int d_root = __shfl_sync(kFull, root, donor);
     const int d_tl = __shfl_sync(kFull, tl, donor);
     const int w = (int)wmax;
     if (thief) {
-      want = d_want; out = d_out != 0; base = d_base; slot = d_slot; root = d_root; tl = d_tl;
+      want = d_want; out = (d_out & 1) != 0; prun = PS && (d_out & 2) != 0; base = d_base; slot = d_slot;
+      root = d_root; tl = d_tl;
       pos = p0 + (int)((long long)w * (rank + 1) / parts);
       end = p0 + (int)((long long)w * (rank + 2) / parts);
     }
@@ -871,7 +927,7 @@ struct Searcher {
 // Persistent search: warps claim root tiles from one work queue covering
 // every query of the launch, switch their per-warp query copy when a tile
 // belongs to another query, and add each query's count to counts[q].
-template <int K, bool ENUM, bool EXACT>
+template <int K, bool ENUM, bool EXACT, bool PS>
 __global__ void __launch_bounds__(kBlock, min_blocks(K))
 search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const LaunchArgs la,
               const __grid_constant__ EnumArgs ea) {
@@ -882,7 +938,7 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
   if (lane < K) sm.nb[lane] = 0;
   if (lane == 0) { sm.halt = 0; sm.cur_q = 0; }
   __syncwarp();
-  Searcher<K, ENUM, EXACT> S(g, sm.q.plan, ea, la, sm, lane);
+  Searcher<K, ENUM, EXACT, PS> S(g, sm.q.plan, ea, la, sm, lane);
   int cur_q = -1;
   auto flush = [&]() {
     if (cur_q >= 0) {
@@ -981,7 +1037,7 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
 
 // The shared-memory attribute belongs to the function on the current
 // device, so it is set once per device (bit d of the mask: device d).
-template <int K, bool ENUM, bool EXACT>
+template <int K, bool ENUM, bool EXACT, bool PS>
 int setup_k() {
   static std::atomic<unsigned long long> done{0ull};
   int dev = 0;
@@ -989,11 +1045,11 @@ int setup_k() {
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
   if (bit && (done.load(std::memory_order_acquire) & bit)) return 0;
-  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT, PS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(kWarps * sizeof(WarpSmem<K>)));
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
 #ifdef EVX_CARVEOUT
-  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT, PS>, cudaFuncAttributePreferredSharedMemoryCarveout,
                            EVX_CARVEOUT);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(carveout)");
 #endif
@@ -1001,20 +1057,20 @@ int setup_k() {
   return 0;
 }
 
-template <int K, bool ENUM, bool EXACT>
+template <int K, bool ENUM, bool EXACT, bool PS>
 int launch_k(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, const EnumArgs &ea, int grid,
              cudaStream_t s) {
-  int rc = setup_k<K, ENUM, EXACT>();
+  int rc = setup_k<K, ENUM, EXACT, PS>();
   if (rc) return rc;
-  search_kernel<K, ENUM, EXACT><<<grid, kBlock, kWarps * sizeof(WarpSmem<K>), s>>>(g, q0, la, ea);
+  search_kernel<K, ENUM, EXACT, PS><<<grid, kBlock, kWarps * sizeof(WarpSmem<K>), s>>>(g, q0, la, ea);
   return 0;
 }
 
-template <int K, bool ENUM, bool EXACT>
+template <int K, bool ENUM, bool EXACT, bool PS>
 int occ_k(int *bps) {
-  int rc = setup_k<K, ENUM, EXACT>();
+  int rc = setup_k<K, ENUM, EXACT, PS>();
   if (rc) return rc;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, search_kernel<K, ENUM, EXACT>, kBlock,
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, search_kernel<K, ENUM, EXACT, PS>, kBlock,
                                                                 kWarps * sizeof(WarpSmem<K>));
   return e == cudaSuccess ? 0 : cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
 }
@@ -1038,18 +1094,37 @@ constexpr int kSingleTileRoots = 64;
 
 }  // namespace
 
-// single-query launches: exact motif size, count or enumerate
+// single-query launches: exact motif size, count or enumerate, with or
+// without the pair-run walk (PS: compiled out where no level needs it)
+#define EVX_K_CASE(FN, KK, ...)                                                      \
+  case KK:                                                                           \
+    if (enumerate) return ps ? FN<KK, true, true, true>(__VA_ARGS__) : FN<KK, true, true, false>(__VA_ARGS__); \
+    return ps ? FN<KK, false, true, true>(__VA_ARGS__) : FN<KK, false, true, false>(__VA_ARGS__);
 #define EVX_K_DISPATCH(FN, ...)                                        \
   switch (k) {                                                         \
-    case 2: return enumerate ? FN<2, true, true>(__VA_ARGS__) : FN<2, false, true>(__VA_ARGS__); \
-    case 3: return enumerate ? FN<3, true, true>(__VA_ARGS__) : FN<3, false, true>(__VA_ARGS__); \
-    case 4: return enumerate ? FN<4, true, true>(__VA_ARGS__) : FN<4, false, true>(__VA_ARGS__); \
-    case 5: return enumerate ? FN<5, true, true>(__VA_ARGS__) : FN<5, false, true>(__VA_ARGS__); \
-    case 6: return enumerate ? FN<6, true, true>(__VA_ARGS__) : FN<6, false, true>(__VA_ARGS__); \
-    case 7: return enumerate ? FN<7, true, true>(__VA_ARGS__) : FN<7, false, true>(__VA_ARGS__); \
-    case 8: return enumerate ? FN<8, true, true>(__VA_ARGS__) : FN<8, false, true>(__VA_ARGS__); \
+    EVX_K_CASE(FN, 2, __VA_ARGS__)                                     \
+    EVX_K_CASE(FN, 3, __VA_ARGS__)                                     \
+    EVX_K_CASE(FN, 4, __VA_ARGS__)                                     \
+    EVX_K_CASE(FN, 5, __VA_ARGS__)                                     \
+    EVX_K_CASE(FN, 6, __VA_ARGS__)                                     \
+    EVX_K_CASE(FN, 7, __VA_ARGS__)                                     \
+    EVX_K_CASE(FN, 8, __VA_ARGS__)                                     \
     default: return fail(EVX_ERR_INVALID, "motif edge count out of range");          \
   }
+
+// Whether a query walks a pair run at some level: an edge between two nodes
+// mapped before it that is scanned (every level before the last; the last
+// one only when enumerating: a counted closing last edge takes range
+// arithmetic instead).
+bool plan_pair_scan(const MotifPlan &plan, int qflags, bool enumerate) {
+  if (!(qflags & kQPairScan)) return false;
+  for (int l = 0; l <= plan.k - 2; l++) {
+    if (plan_kind(plan.info[l]) != 2) continue;
+    if (l < plan.k - 2 || enumerate) return true;
+  }
+  return false;
+}
+
 int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &args, int grid, int block,
                   cudaStream_t stream) {
   (void)block;
@@ -1072,10 +1147,11 @@ int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &a
   ea.exact_total = args.exact_total;
   ea.stop = args.stop;
   ea.count = args.count;
+  const bool ps = plan_pair_scan(plan, q0.flags, enumerate);
   EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
 }
 
-int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int k, int grid,
+int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int k, bool ps, int grid,
                  cudaStream_t stream) {
   const bool enumerate = false;
   EnumArgs ea;
@@ -1083,12 +1159,12 @@ int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, 
   EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
 }
 
-int search_occupancy(int k, bool enumerate, int block, int *blocks_per_sm) {
+int search_occupancy(int k, bool enumerate, bool ps, int block, int *blocks_per_sm) {
   (void)block;
   EVX_K_DISPATCH(occ_k, blocks_per_sm)
 }
 
-int table_occupancy(int k, int *blocks_per_sm) {
+int table_occupancy(int k, bool ps, int *blocks_per_sm) {
   const bool enumerate = false;
   EVX_K_DISPATCH(occ_k, blocks_per_sm)
 }

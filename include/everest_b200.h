@@ -59,6 +59,12 @@ extern "C" {
  * arithmetic (window length minus the entries of the pairs to nodes already
  * mapped).  This keeps the scan instead. */
 #define EVX_FLAG_NEW_SCAN 128u
+/* A motif edge between two nodes mapped before it (not counted by range
+ * arithmetic) walks the run of its static edge (u, v) in the pair index:
+ * only the matching edges, after the previous edge and inside the window.
+ * This scans the shorter of out(u) / in(v) instead, as the reference does
+ * (system/templates/common/resolveMi.snp:9-28). */
+#define EVX_FLAG_LIST_SCAN 256u
 
 typedef struct evx_graph evx_graph;   /* a graph resident on one device */
 typedef struct evx_worker evx_worker; /* per-device search worker */

@@ -70,6 +70,10 @@ def test_golden_small_graph_counts(golden, small_graphs, worker):
                 got4 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
                                  flags=capi.FLAG_CLOSING_SCAN)
                 assert got4 == c["count"], (gname, c["motif"], c["delta"], got4, "closing scan")
+            if n % 6 == 2:  # mid-level closing edges scanned in the shorter list on a subset
+                got6 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
+                                 flags=capi.FLAG_LIST_SCAN)
+                assert got6 == c["count"], (gname, c["motif"], c["delta"], got6, "list scan")
             if n % 7 == 0:  # the scanning last level on a subset
                 got2 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
                                  flags=capi.FLAG_NO_PAIR_INDEX)
@@ -131,11 +135,13 @@ def test_random_tiny_vs_brute_force(worker):
         want = len(O.brute_force(u, v, t, mu, mv, delta))
         dg = device_graph(u, v, t)
         for flags in (0, capi.FLAG_NO_STEAL, capi.FLAG_NO_PAIR_INDEX, capi.FLAG_PAIR_DIR, capi.FLAG_CLOSING_SCAN,
-                      capi.FLAG_NO_CLOSING_PRUNE, capi.FLAG_NO_CLOSING_PRUNE | capi.FLAG_NO_PAIR_INDEX):
+                      capi.FLAG_NO_CLOSING_PRUNE, capi.FLAG_NO_CLOSING_PRUNE | capi.FLAG_NO_PAIR_INDEX,
+                      capi.FLAG_LIST_SCAN, capi.FLAG_LIST_SCAN | capi.FLAG_NO_STEAL):
             assert gpu_count(worker, dg, mu, mv, delta, flags=flags) == want, (trial, pat, delta, flags)
         strict = len(O.brute_force(u, v, t, mu, mv, delta, strict_ts=True))
         assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS) == strict
         assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS | capi.FLAG_CLOSING_SCAN) == strict
+        assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS | capi.FLAG_LIST_SCAN) == strict
         dg.free()
 
 
@@ -251,6 +257,31 @@ def test_enumeration_cap_rule(small_graphs, worker):
     worker.take(dg, mu, mv, delta, 0, -1, cap, capi.FLAG_EXACT_TOTAL)
     assert worker.run() == total
     dg.free()
+
+
+def test_enumeration_random_tiny_vs_brute_force(worker):
+    """Enumerated rows equal brute force's on random tiny graphs, for motifs
+    whose middle edges join mapped nodes (pair-run walks) and otherwise, with
+    the pair-run walk on and off."""
+    rng = np.random.default_rng(321)
+    pats = [([0, 1, 0], [1, 0, 1]), ([0, 0, 1], [1, 1, 0]), ([0, 1, 1, 2], [1, 2, 0, 0]),
+            ([0, 1, 2, 1], [1, 2, 0, 2]), ([0, 1, 2, 3], [1, 2, 3, 0]), ([0, 1, 1, 0], [1, 0, 0, 1])]
+    for trial in range(60):
+        E = int(rng.integers(0, 30))
+        V = int(rng.integers(2, 6))
+        u = rng.integers(0, V, E).astype(np.int32)
+        v = rng.integers(0, V, E).astype(np.int32)
+        t = np.sort(rng.integers(0, 12, E)).astype(np.int32)
+        mu, mv = pats[trial % len(pats)]
+        delta = int(rng.integers(0, 9))
+        want = sorted(map(tuple, O.brute_force(u, v, t, mu, mv, delta)))
+        dg = device_graph(u, v, t)
+        for flags in (0, capi.FLAG_LIST_SCAN, capi.FLAG_NO_STEAL):
+            worker.take(dg, mu, mv, delta, 0, -1, len(want) + 4, flags)
+            assert worker.run() == len(want), (trial, mu, mv, delta, flags)
+            got = sorted(map(tuple, worker.enum_rows(len(want) + 4).tolist()))
+            assert got == want, (trial, mu, mv, delta, flags)
+        dg.free()
 
 
 def test_enumeration_matches_count_zipf(worker):
