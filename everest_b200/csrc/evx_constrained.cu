@@ -172,13 +172,29 @@ __device__ __forceinline__ int first_eid_after(const int4 *__restrict__ recs, in
   return lo;
 }
 
+// Per-lane search state of one warp, indexed [level][lane]: each lane keeps
+// its own column, so the dynamically indexed levels cost shared-memory
+// accesses (conflict-free: 32 lanes, 32 consecutive words) instead of a
+// local-memory stack.
+template <int K>
+struct ConsWarpState {
+  int m[K + 1][32];             // graph node of each motif node
+  int eid[K][32], et[K][32];    // matched edge and its time per motif edge (anti: none)
+  int pos[K][32], endp[K][32], tlv[K][32];
+};
+
 template <int K, bool ENUM>
 __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView g,
                                                                  const __grid_constant__ ConsSearch s) {
   const int lane = threadIdx.x & 31;
-  int m[K + 1];             // graph node of each motif node
-  int eid[K], et[K];        // matched edge and its time per motif edge (anti: none)
-  int pos[K], endp[K], tlv[K];
+  __shared__ ConsWarpState<K> wst[kConsBlock / 32];
+  ConsWarpState<K> &W = wst[threadIdx.x >> 5];
+  auto m = [&](int i) -> int & { return W.m[i][lane]; };
+  auto eid = [&](int i) -> int & { return W.eid[i][lane]; };
+  auto et = [&](int i) -> int & { return W.et[i][lane]; };
+  auto pos = [&](int i) -> int & { return W.pos[i][lane]; };
+  auto endp = [&](int i) -> int & { return W.endp[i][lane]; };
+  auto tlv = [&](int i) -> int & { return W.tlv[i][lane]; };
   unsigned useout = 0;      // bit j: motif edge j scans an out-list
   int j = 0;                // motif edge being scanned; 0 = between roots
   bool done = false;        // no roots left for this lane
@@ -191,10 +207,10 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
     const int pr = s.prev_real[jj];
     int tl;
     if (s.has_temporal) {
-      const int gap = et[pr] + s.temporal[jj - 1];
-      tl = (jj >= 2 && et[0] + s.delta < gap) ? et[0] + s.delta : gap;
+      const int gap = et(pr) + s.temporal[jj - 1];
+      tl = (jj >= 2 && et(0) + s.delta < gap) ? et(0) + s.delta : gap;
     } else {
-      tl = et[0] + s.delta;
+      tl = et(0) + s.delta;
     }
     bool out;
     int lo, hi;
@@ -203,20 +219,20 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
     } else if (kind == 0) {
       out = false;
     } else {
-      const int4 ra = __ldg(g.node_rng + m[a]), rb = __ldg(g.node_rng + m[b]);
+      const int4 ra = __ldg(g.node_rng + m(a)), rb = __ldg(g.node_rng + m(b));
       out = !(rb.w - rb.z < ra.y - ra.x);  // the shorter list; ties go to out(a)
     }
     if (out) {
-      const int4 r = __ldg(g.node_rng + m[a]);
+      const int4 r = __ldg(g.node_rng + m(a));
       lo = r.x; hi = r.y;
     } else {
-      const int4 r = __ldg(g.node_rng + m[b]);
+      const int4 r = __ldg(g.node_rng + m(b));
       lo = r.z; hi = r.w;
     }
-    lo = first_eid_after(out ? g.out_rec : g.in_rec, lo, hi, eid[pr]);
-    pos[jj] = lo;
-    endp[jj] = hi;
-    tlv[jj] = tl;
+    lo = first_eid_after(out ? g.out_rec : g.in_rec, lo, hi, eid(pr));
+    pos(jj) = lo;
+    endp(jj) = hi;
+    tlv(jj) = tl;
     useout = out ? (useout | (1u << jj)) : (useout & ~(1u << jj));
     j = jj;
   };
@@ -245,10 +261,10 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
           }
           if (ok && s.edge_ok) ok = __ldg(s.edge_ok + r) != 0;
           if (ok) {
-            m[0] = e.x;
-            m[1] = e.y;
-            eid[0] = r;
-            et[0] = e.z;
+            m(0) = e.x;
+            m(1) = e.y;
+            eid(0) = r;
+            et(0) = e.z;
             open(1);
           }
         }
@@ -262,11 +278,11 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
     const int kind = plan_kind(w), a = plan_a(w), b = plan_b(w), nm = plan_nm(w);
     const bool out = (useout >> j) & 1;
     const int4 *__restrict__ recs = out ? g.out_rec : g.in_rec;
-    const int want = kind == 2 ? (out ? m[b] : m[a]) : -1;
+    const int want = kind == 2 ? (out ? m(b) : m(a)) : -1;
     const bool anti = (s.anti_mask >> j) & 1;
     const bool last = (j == K - 1);
-    const int tl = tlv[j], hi = endp[j];
-    int p = pos[j];
+    const int tl = tlv(j), hi = endp(j);
+    int p = pos(j);
     int found = -1, fnode = 0, ft = 0;
     for (; p < hi; p++) {
       const int4 r = __ldg(recs + p);
@@ -278,7 +294,7 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
         ok = true;
 #pragma unroll
         for (int q = 0; q < K + 1; q++)
-          if (q < nm && m[q] == r.y) ok = false;
+          if (q < nm && m(q) == r.y) ok = false;
         if (ok && s.node_ok) ok = ((__ldg(s.node_ok + r.y) >> nm) & 1) != 0;
       }
       if (ok && s.edge_ok) ok = __ldg(s.edge_ok + r.x) != 0;
@@ -287,7 +303,7 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
         bool pass = true;
         if (s.has_filter) {
           pass = prog_eval(s.filter, [&](int i) -> long long {
-                   const int e = i == K - 1 ? r.x : eid[i];
+                   const int e = i == K - 1 ? r.x : eid(i);
                    return e < 0 ? 0 : __ldg(s.edge_feat + e);
                  }) != 0;
         }
@@ -297,7 +313,7 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
           if ((long long)slot < s.cap) {
             int *row = s.rows + slot * (unsigned long long)K;
 #pragma unroll
-            for (int q = 0; q < K - 1; q++) row[q] = eid[q] < 0 ? -1 : __ldg(g.euid + eid[q]);
+            for (int q = 0; q < K - 1; q++) row[q] = eid(q) < 0 ? -1 : __ldg(g.euid + eid(q));
             row[K - 1] = __ldg(g.euid + r.x);
           }
           if ((long long)slot >= s.cap - 1 && !s.exact_total) *(volatile int *)s.stop = 1;
@@ -312,15 +328,15 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
       p++;
       break;
     }
-    pos[j] = p;
+    pos(j) = p;
     if (!last && anti && found < 0) {
-      eid[j] = -1;  // the edge that must not exist does not: go on
-      et[j] = 0;
+      eid(j) = -1;  // the edge that must not exist does not: go on
+      et(j) = 0;
       open(j + 1);
     } else if (!last && !anti && found >= 0) {
-      eid[j] = found;
-      et[j] = ft;
-      if (kind != 2) m[nm] = fnode;
+      eid(j) = found;
+      et(j) = ft;
+      if (kind != 2) m(nm) = fnode;
       open(j + 1);
     } else {
       // window exhausted, or an anti-edge exists: back to the previous real
