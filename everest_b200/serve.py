@@ -14,11 +14,15 @@ The reference answers one query at a time and re-uploads the graph for each
     (cap x k x 4 bytes plus a reserve) and an enumeration slot is free;
 * completed work is detected without blocking (CUDA event queries), futures
   are resolved and each request's latency (submit -> result) is recorded;
-* an optional work limit bounds any one query (work = adjacency records
-  examined inside their time windows, fixed by the graph and the query): a
-  query past it is stopped on the device and resolved with
-  ``Result.limited`` set and no count (an enumeration keeps the rows it
-  wrote); every other result is exact.
+* an optional work limit keeps heavy queries out of the shared batches
+  (work = adjacency records examined inside their time windows, fixed by
+  the graph and the query): a query past it is stopped on the device and
+  re-queued for a heavy slot, a worker that runs one query at a time with no
+  limit on a fraction of the SMs while other work is about, so that it
+  overlaps the batches instead of holding them back.  Its result is exact
+  like every other (``Result.requeued`` says it took that route).  With
+  ``heavy_slots=0`` a query past the limit is resolved with
+  ``Result.limited`` set and no count instead.
 
 Results are independent of the mix: every query keeps its own counters in
 the batch (one per query) or its own worker.
@@ -57,14 +61,16 @@ class Result:
     count: Optional[int]
     rows: Optional[np.ndarray] = None
     latency_s: float = 0.0
-    limited: bool = False  # stopped at the work limit (count is None)
+    limited: bool = False   # stopped at the work limit and not re-run (count is None)
+    requeued: bool = False  # passed the work limit and was re-run on a heavy slot
 
 
 class Server:
     def __init__(self, device: int = 0, max_batch: int = 64, inflight_batches: int = 2,
                  enum_slots: int = 2, mem_reserve: int = 1 << 30, idle_sleep_s: float = 50e-6,
                  backend=None, limit: int = 0, use_graph: bool = False, tile_roots: int = 64,
-                 enum_blocks_per_sm: int = 2, batch_share: float = 1.0):
+                 enum_blocks_per_sm: int = 2, batch_share: float = 1.0, heavy_slots: int = 2,
+                 heavy_blocks_per_sm: int = 2):
         # backend: the module providing Batch, Worker, DeviceGraph and
         # device_mem_info (the C-ABI binding; tests substitute a fake)
         self.be = backend if backend is not None else capi
@@ -107,6 +113,13 @@ class Server:
         # room; with no count work about, on the whole GPU
         self.enum_blocks_per_sm = int(enum_blocks_per_sm)
         self.enum_reqs: List[Optional[Request]] = [None] * enum_slots
+        # heavy slots: queries that passed the work limit, re-run without it
+        self.heavy_q: "collections.deque[Request]" = collections.deque()
+        self.heavy_workers = [capi_.Worker(device) for _ in range(heavy_slots if self.limit else 0)]
+        self.heavy_reqs: List[Optional[Request]] = [None] * len(self.heavy_workers)
+        self.heavy_t0: List[float] = [0.0] * len(self.heavy_workers)
+        self.heavy_blocks_per_sm = int(heavy_blocks_per_sm)
+        self.requeued = 0
         self.latencies: List[float] = []
         # (kind, launch time, completion time, queries) of every launch
         self.launch_log: List[tuple] = []
@@ -157,7 +170,8 @@ class Server:
     def stats(self) -> dict:
         lat = np.array(self.latencies) if self.latencies else np.zeros(1)
         span = (self.last_done - self.first_submit) if (self.last_done and self.first_submit) else 0.0
-        return {"completed": self.completed, "limited": self.limited, "batches": self.batches_launched,
+        return {"completed": self.completed, "limited": self.limited, "requeued": self.requeued,
+                "batches": self.batches_launched,
                 "queries_per_s": self.completed / span if span > 0 else 0.0,
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                 "p999_ms": float(np.percentile(lat, 99.9) * 1e3), "max_ms": float(lat.max() * 1e3),
@@ -168,7 +182,7 @@ class Server:
         t0 = time.time()
         while True:
             with self.lock:
-                busy = (self.count_q or self.enum_q or any(self.batch_reqs) or any(self.enum_reqs))
+                busy = self._busy()
             if not busy:
                 return
             if self.error:
@@ -184,7 +198,7 @@ class Server:
         self.thread.join(timeout=60)
         for b in self.batches:
             b.close()
-        for w in self.enum_workers:
+        for w in self.enum_workers + self.heavy_workers:
             w.close()
         for g in self.graphs.values():
             if hasattr(g, "free"):
@@ -192,6 +206,16 @@ class Server:
         self.graphs.clear()
 
     # ------------------------------------------------------------ loop --
+    def _busy(self) -> bool:
+        return bool(self.count_q or self.enum_q or self.heavy_q or any(self.batch_reqs) or any(self.enum_reqs)
+                    or any(self.heavy_reqs))
+
+    def _requeue(self, reqs: List[Request]) -> None:
+        """Queries past the work limit: run them again on a heavy slot (the
+        caller holds the lock)."""
+        self.requeued += len(reqs)
+        self.heavy_q.extend(reqs)
+
     def _finish(self, r: Request, res: Result) -> None:
         now = time.perf_counter()
         res.latency_s = now - r.submitted
@@ -209,10 +233,14 @@ class Server:
                 self.launch_log.append(("batch", self.batch_t0[i], time.perf_counter(), len(reqs)))
                 counts = b.result()
                 b.clear()
-                self.batch_reqs[i] = None
+                again = [r for r, c in zip(reqs, counts) if c == capi.LIMITED] if self.heavy_workers else []
+                with self.lock:  # re-queued and released together: drain() always sees them
+                    self._requeue(again)
+                    self.batch_reqs[i] = None
                 for r, c in zip(reqs, counts):
                     lim = c == capi.LIMITED
-                    self._finish(r, Result(None if lim else c, limited=lim))
+                    if not (lim and self.heavy_workers):
+                        self._finish(r, Result(None if lim else c, limited=lim))
                 progressed = True
         for i, w in enumerate(self.enum_workers):
             r = self.enum_reqs[i]
@@ -223,9 +251,21 @@ class Server:
                     c, lim = w.result(), False
                 except capi.LimitExceeded:
                     c, lim = None, True
+                with self.lock:
+                    self._requeue([r] if (lim and self.heavy_workers) else [])
+                    self.enum_reqs[i] = None
+                if not (lim and self.heavy_workers):
+                    rows = w.enum_rows(r.enum_cap) if r.enum_cap > 0 else None
+                    self._finish(r, Result(c, rows, limited=lim))
+                progressed = True
+        for i, w in enumerate(self.heavy_workers):
+            r = self.heavy_reqs[i]
+            if r is not None and w.done():
+                self.launch_log.append(("heavy", self.heavy_t0[i], time.perf_counter(), 1))
+                c = w.result()
                 rows = w.enum_rows(r.enum_cap) if r.enum_cap > 0 else None
-                self.enum_reqs[i] = None
-                self._finish(r, Result(c, rows, limited=lim))
+                self.heavy_reqs[i] = None
+                self._finish(r, Result(c, rows, requeued=True))
                 progressed = True
         return progressed
 
@@ -289,6 +329,36 @@ class Server:
             w.launch()
             self.enum_t0[i] = time.perf_counter()
             progressed = True
+        # heavy queries: one per slot, no work limit, on a fraction of the SMs
+        # while other work is queued or running (the whole GPU otherwise)
+        for i, w in enumerate(self.heavy_workers):
+            if self.heavy_reqs[i] is not None:
+                continue
+            with self.lock:
+                if not self.heavy_q:
+                    break
+                r = self.heavy_q[0]
+            if r.enum_cap > 0:
+                need = r.enum_cap * len(r.mu) * 4
+                free, _ = self.be.device_mem_info(self.device)
+                if need + self.mem_reserve > free:
+                    break
+            with self.lock:
+                self.heavy_q.popleft()
+                self.heavy_reqs[i] = r
+            if r.constraints is not None:
+                w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags,
+                       constraints=r.constraints)
+            else:
+                w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags)
+            if hasattr(w, "set_tuning"):
+                busy = bool(self.count_q or self.enum_q) or any(x is not None for x in self.batch_reqs) \
+                    or any(x is not None for x in self.enum_reqs)
+                w.set_tuning(block=128, blocks_per_sm=self.heavy_blocks_per_sm if busy else 0,
+                             roots_per_fetch=32, steal_interval=16, min_split=2)
+            w.launch()
+            self.heavy_t0[i] = time.perf_counter()
+            progressed = True
         return progressed
 
     def _loop(self) -> None:
@@ -297,7 +367,7 @@ class Server:
                 with self.cv:
                     if not self.running:
                         return
-                    idle = not (self.count_q or self.enum_q or any(self.batch_reqs) or any(self.enum_reqs))
+                    idle = not self._busy()
                     if idle:
                         self.cv.wait(timeout=0.05)
                         continue
@@ -311,6 +381,7 @@ class Server:
                 pending = list(self.count_q) + list(self.enum_q)
                 pending += [r for reqs in self.batch_reqs if reqs for r in reqs]
                 pending += [r for r in self.enum_reqs if r]
+                pending += list(self.heavy_q) + [r for r in self.heavy_reqs if r]
             for r in pending:
                 if not r.future.done():
                     r.future.set_exception(e)

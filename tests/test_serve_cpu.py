@@ -82,6 +82,7 @@ class FakeBackend:
 
             def take(self, g, mu, mv, d, beg, end, cap, flags, constraints=None):
                 self.args = (g, mu, mv, d, cap)
+                self.roots = (beg, end)
                 self.cons = constraints
 
             def launch(self):
@@ -96,7 +97,15 @@ class FakeBackend:
                     self.total = O.count_constrained(be.graphs[g], mu, mv, d, self.cons.to_struct(), nf, ef)
                     self.rows = None
                 else:
-                    self.rows, self.total = O.enumerate_rows(be.graphs[g], mu, mv, d, cap)
+                    gr = be.graphs[g]
+                    beg, end = self.roots
+                    top = O.default_roots(gr, len(mu))[1]
+                    hi = top if end < 0 else min(end, top)
+                    roots = (beg, max(beg, hi))
+                    if cap > 0:
+                        self.rows, self.total = O.enumerate_rows(gr, mu, mv, d, cap, roots=roots)
+                    else:
+                        self.rows, self.total = None, O.count(gr, mu, mv, d, roots=roots)[0]
                 self.t_done = time.perf_counter() + 0.003
 
             def done(self):
@@ -176,7 +185,9 @@ def test_root_ranges_and_count_limit(graph):
         hi = O.default_roots(graph, len(mu))[1] if end < 0 else min(end, O.default_roots(graph, len(mu))[1])
         exact.append(O.count(graph, mu, mv, d, roots=(beg, hi))[0])
     limit = sorted(exact)[-2]  # the largest query passes it, the others do not
-    srv = serve.Server(max_batch=4, inflight_batches=1, enum_slots=1, mem_reserve=0, backend=be, limit=limit)
+    # without heavy slots a query past the limit comes back flagged, with no count
+    srv = serve.Server(max_batch=4, inflight_batches=1, enum_slots=1, mem_reserve=0, backend=be, limit=limit,
+                       heavy_slots=0)
     srv.add_graph("g", "g")
     futs = [srv.submit("g", mu, mv, d, beg=beg, end=end) for mu, mv, d, beg, end in qs]
     srv.drain(60)
@@ -187,6 +198,20 @@ def test_root_ranges_and_count_limit(graph):
         else:
             assert not r.limited and r.count == c
     assert srv.stats()["limited"] == sum(c > limit for c in exact) == 1
+    srv.close()
+    # with heavy slots (the default) it is re-run without the limit: every
+    # query gets its exact count
+    srv = serve.Server(max_batch=4, inflight_batches=1, enum_slots=1, mem_reserve=0, backend=be, limit=limit)
+    srv.add_graph("g", "g")
+    futs = [srv.submit("g", mu, mv, d, beg=beg, end=end) for mu, mv, d, beg, end in qs]
+    srv.drain(60)
+    for f, c in zip(futs, exact):
+        r = f.result(1)
+        assert not r.limited and r.count == c
+        assert r.requeued == (c > limit)
+    st = srv.stats()
+    assert st["limited"] == 0 and st["requeued"] == 1 and st["completed"] == len(qs)
+    assert any(k == "heavy" for k, *_ in srv.launch_log)
     srv.close()
 
 
