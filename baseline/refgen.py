@@ -245,6 +245,13 @@ class RefGraph:
         self.num_edges = E
 
     @classmethod
+    def from_host_graph(cls, h) -> "RefGraph":
+        """From the reference's HostGraphData arrays as this library builds
+        them (everest_b200.capi.HostGraph: relabeled vertices, Eg AoS)."""
+        eg = np.asarray(h.eg, np.int32).reshape(-1, 3)
+        return cls(eg[:, 0], eg[:, 1], eg[:, 2], h.in_v, h.in_r, h.out_v, h.out_r, h.num_vertices)
+
+    @classmethod
     def from_oracle_graph(cls, g) -> "RefGraph":
         """From an oracle.Graph (sorted edges plus stable CSR by edge id)."""
         return cls(g.u, g.v, g.t, g.in_eid[:g.E], g.in_off, g.out_eid[:g.E], g.out_off, g.V)

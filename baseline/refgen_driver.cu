@@ -1,7 +1,8 @@
 // Runs the search the reference generates for one query -- the file that
 // system/tmine/KernelGen.py:112-151 writes with warpCentric, warpBalancing
-// and tailExpansion on, the configuration Everest ships -- built for
-// sm_100a, through its own GPUWorker (getWorker / take / run,
+// and tailExpansion on, the configuration Everest ships -- or one of its
+// legacy ablation plugins (plugins/GPUWorker*.cu), built for sm_100a,
+// through its own GPUWorker (getWorker / take / run,
 // system/templates/GPUWorker/*.snp).  A comparator for timing and a
 // full-size parity check; the library of this repository never links it.
 //
@@ -33,7 +34,11 @@ void put_error(char *err, int errlen, const std::string &s) {
 }  // namespace
 
 // Upload the reference's HostGraphData arrays (Eg AoS {u, v, t}, in/out edge
-// lists, in/out offsets; src/core/gpu/data.cu:124-348) to device 0.
+// lists, in/out offsets; src/core/gpu/data.cu:124-348) to device 0.  Every
+// array gets kPad zeroed entries past its end: the legacy U0 and U1 plugins
+// read Eg[tid] before they check tid < work, for tids up to one block (96)
+// past the last root.
+constexpr size_t kPad = 256;
 extern "C" int refgen_graph_upload(const int *eg_aos, int num_edges, const int *in_v, const int *in_r,
                                    const int *out_v, const int *out_r, int num_vertices, void **out,
                                    char *err, int errlen) {
@@ -41,13 +46,18 @@ extern "C" int refgen_graph_upload(const int *eg_aos, int num_edges, const int *
   try {
     g->num_edges = num_edges;
     g->num_vertices = num_vertices;
-    const size_t e = (size_t)(num_edges > 0 ? num_edges : 1), nv = (size_t)num_vertices + 1;
+    const size_t e = (size_t)(num_edges > 0 ? num_edges : 1) + kPad, nv = (size_t)num_vertices + 1 + kPad;
     gpuErrchk(cudaSetDevice(0));
     gpuErrchk(cudaMalloc(&g->eg, sizeof(corelib::TemporalEdge) * e));
     gpuErrchk(cudaMalloc(&g->in_v, sizeof(int) * e));
     gpuErrchk(cudaMalloc(&g->out_v, sizeof(int) * e));
     gpuErrchk(cudaMalloc(&g->in_r, sizeof(int) * nv));
     gpuErrchk(cudaMalloc(&g->out_r, sizeof(int) * nv));
+    gpuErrchk(cudaMemset(g->eg, 0, sizeof(corelib::TemporalEdge) * e));
+    gpuErrchk(cudaMemset(g->in_v, 0, sizeof(int) * e));
+    gpuErrchk(cudaMemset(g->out_v, 0, sizeof(int) * e));
+    gpuErrchk(cudaMemset(g->in_r, 0, sizeof(int) * nv));
+    gpuErrchk(cudaMemset(g->out_r, 0, sizeof(int) * nv));
     gpuErrchk(cudaMemcpy(g->eg, eg_aos, sizeof(corelib::TemporalEdge) * (size_t)num_edges, cudaMemcpyHostToDevice));
     gpuErrchk(cudaMemcpy(g->in_v, in_v, sizeof(int) * (size_t)num_edges, cudaMemcpyHostToDevice));
     gpuErrchk(cudaMemcpy(g->out_v, out_v, sizeof(int) * (size_t)num_edges, cudaMemcpyHostToDevice));
@@ -103,13 +113,20 @@ extern "C" int refgen_count(void *h, const int *mu, const int *mv, int k, int de
     m.arrV = m.io == 1 ? g->out_v : g->in_v;
     mi.push_back(m);
   }
+  // motif edges {u, v, t} in time order (HostMotifData::edges; the legacy
+  // U0 plugin reads them)
+  std::vector<corelib::TemporalEdge> em;
+  for (int i = 0; i < k; i++) em.push_back({mu[i], mv[i], i + 1});
   corelib::MotifEdgeInfoV1 *mi_d = nullptr;
+  corelib::TemporalEdge *em_d = nullptr;
   corelib::GPUWorker *w = nullptr;
   int rc = 0;
   try {
     gpuErrchk(cudaSetDevice(0));
     gpuErrchk(cudaMalloc(&mi_d, sizeof(corelib::MotifEdgeInfoV1) * mi.size()));
     gpuErrchk(cudaMemcpy(mi_d, mi.data(), sizeof(corelib::MotifEdgeInfoV1) * mi.size(), cudaMemcpyHostToDevice));
+    gpuErrchk(cudaMalloc(&em_d, sizeof(corelib::TemporalEdge) * em.size()));
+    gpuErrchk(cudaMemcpy(em_d, em.data(), sizeof(corelib::TemporalEdge) * em.size(), cudaMemcpyHostToDevice));
     corelib::data::DeviceJobData dd;
     dd.device = 0;
     dd.graphNumEdges = (size_t)g->num_edges;
@@ -120,6 +137,7 @@ extern "C" int refgen_count(void *h, const int *mu, const int *mv, int k, int de
     dd.motifNumEdges = (size_t)k;
     dd.motifNumVertices = (size_t)node_max + 1;
     dd.minfo_d = mi_d;
+    dd.em_d = em_d;
     corelib::data::MineJob job;
     job.device = 0;
     job.beg = beg < 0 ? 0 : beg;
@@ -147,5 +165,6 @@ extern "C" int refgen_count(void *h, const int *mu, const int *mv, int k, int de
   }
   if (rc == 0) delete w;  // its destructor throws on a CUDA error; leak it then
   cudaFree(mi_d);
+  cudaFree(em_d);
   return rc;
 }

@@ -1,8 +1,9 @@
 // Stand-ins for the two reference headers that the generated per-query
 // search file includes (include/helpers.cuh, include/data.h), so that the
-// file KernelGen writes (system/tmine/KernelGen.py:112-151) compiles for
-// sm_100a without the reference's corelib host library, which needs Boost,
-// range-v3 and a network fetch to build.
+// file KernelGen writes (system/tmine/KernelGen.py:112-151) and the legacy
+// plugins (plugins/GPUWorker*.cu) compile for sm_100a without the
+// reference's corelib host library, which needs Boost, range-v3 and a
+// network fetch to build.
 //
 // The types keep the reference's field names and meaning:
 //   TemporalEdge            include/data.h:27-29
@@ -84,7 +85,9 @@ struct DeviceJobData {
   const int *Euid_d{nullptr};
   size_t motifNumEdges{0}, motifNumVertices{0};
   const MotifEdgeInfoV1 *minfo_d{nullptr};
+  const TemporalEdge *em_d{nullptr};  // motif edges {u, v, t} (HostMotifData::edges)
   const MotifEdgeInfoV1 *minfo() const { return minfo_d; }
+  const TemporalEdge *Em_d() const { return em_d; }
 };
 struct MineJob {
   int device{-1};
@@ -108,5 +111,7 @@ struct GPUWorker {
   virtual void update_job() = 0;
   virtual std::vector<int> printEnum(int) { return {}; }
   unsigned long long count() const { return count_; }
+  // src/core/cpu/data.cc:556-562: one thread per root of the job
+  int numBlocks() const { return job_ ? (job_->end + sizeBlock_ - 1) / sizeBlock_ : -1; }
 };
 }  // namespace corelib

@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--impl", default="evx", choices=["evx", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the legs beside the headline step (reference GPU kernel, enumeration, "
+                         "batch, serve)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="default launch parameters instead of per-query autotuned ones")
     ap.add_argument("--single-query", type=int, default=-1,
@@ -65,9 +68,10 @@ def parse():
     ap.add_argument("--queries", type=int, default=0, help="batch/serve: number of queries")
     ap.add_argument("--window", type=int, default=0,
                     help="batch/serve: roots per query (a random time window of the edge list)")
-    ap.add_argument("--serve-slots", default="64,2,2,2",
+    ap.add_argument("--serve-slots", default="64,2,2,2,1.0,2,2",
                     help="serve: max queries per batch, batches in flight, enumeration slots, "
-                         "blocks per SM of an enumeration (0 = all)[, share of a batch kernel's blocks]")
+                         "blocks per SM of an enumeration (0 = all), share of a batch kernel's blocks, "
+                         "heavy slots, blocks per SM of a heavy query beside other work")
     ap.add_argument("--limit", type=float, default=1e8,
                     help="batch/serve: work limit per query, in adjacency records examined inside "
                          "their time windows (stopped queries are flagged in both arms)")
@@ -185,53 +189,101 @@ def max_over_ranks(value: float, dist, device=None) -> float:
 
 # --------------------------------------------------------- CPU reference --
 
-def cpu_reference(wname, root_frac, threads):
+CPU_STRIDE = 16        # the CPU legs time every 16th root of each query
+CPU_STRIDE_1T = 256    # the single-thread figure: every 256th root
+
+
+def host_info() -> dict:
+    """Host cores and CPU model of the machine the CPU legs run on."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        usable = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        usable = os.cpu_count() or 1
+    return {"nproc": os.cpu_count() or 1, "usable_cores": usable, "cpu_model": model}
+
+
+def workload_config(wname) -> dict:
+    """The workload the bench line is quoted on (identical in both arms)."""
+    from everest_b200 import synth
+    stats = workload_stats(wname)
+    spec = synth.SPECS[stats["graph"]]
+    return {"workload": "bursty-7.8m-3edge: 1.1M nodes, 7.8M edges, 36 three-edge motifs "
+                        "run separately, delta 86400, count",
+            "graph_edges": spec.num_edges, "graph_vertices": spec.num_nodes,
+            "queries_per_step": len(stats["queries"]),
+            "matches_per_step": sum(r["count"] for r in stats["queries"]),
+            "l2": "GPU arm: flushed before every step (256 MB write); CPU arm: not applicable",
+            "parallelism": "replicas (one GPU per query stream; no data-path collective)"}
+
+
+_cpu_graphs = {}
+
+
+def cpu_reference(wname, stride, threads):
     """Time the reference's own CPU path (host build of its Baseline body)
-    on roots [0, E * root_frac) of every query; returns (matches, seconds,
-    kind)."""
+    over roots 0, stride, 2 stride, ... of every query of the workload (an
+    even sample of the whole time range); returns (matches, seconds, kind,
+    roots sampled per query)."""
     from oracle import oracle as O
     from everest_b200 import synth, workloads
     spec = synth.SPECS[workload_stats(wname)["graph"]]
-    u, v, t = synth.load_or_generate(spec.name)
-    g = O.Graph(u, v, t, spec.num_nodes)
-    S = int(g.E * root_frac)
+    if spec.name not in _cpu_graphs:
+        u, v, t = synth.load_or_generate(spec.name)
+        _cpu_graphs[spec.name] = O.Graph(u, v, t, spec.num_nodes)
+    g = _cpu_graphs[spec.name]
     kind = "reference" if O.ref_lib() is not None else "port"
-    total = 0
+    total, n = 0, 0
     t0 = time.perf_counter()
     for q in workloads.queries(wname):
+        work = max(0, g.E - len(q["mu"]) + 1)
+        n = (work + stride - 1) // stride
         if kind == "reference":
-            total += O.ref_baseline_count(g, q["mu"], q["mv"], q["delta"], roots=(0, S),
-                                          threads=threads)
+            total += O.ref_baseline_count(g, q["mu"], q["mv"], q["delta"], roots=(0, work),
+                                          threads=threads, stride=stride)
         else:
-            total += O.count(g, q["mu"], q["mv"], q["delta"], roots=(0, S), threads=threads)[0]
-    return total, time.perf_counter() - t0, kind, S
+            # the oracle takes contiguous ranges: the same roots one by one
+            total += sum(O.count(g, q["mu"], q["mv"], q["delta"], roots=(r, r + 1), threads=1)[0]
+                         for r in range(0, work, stride))
+    return total, time.perf_counter() - t0, kind, n
+
+
+def cpu_sample_text(stride, threads, n):
+    return (f"every {stride}th root ({n} per query, spread over the whole time range) of each of the 36 "
+            f"queries on the 7.8M-edge graph, {threads} threads; rate = sampled matches / time")
 
 
 def run_reference_arm(args):
     world, rank, local, dist = dist_setup(args.gpus)
     if rank != 0:
         return 0
-    threads = os.cpu_count() or 1
-    frac = 1.0 / 16
+    threads = host_info()["usable_cores"]
     times, matches = [], 0
-    kind, S = "reference", 0
+    kind, n = "reference", 0
     for i in range(args.warmup + args.steps):
-        m, dt, kind, S = cpu_reference(args.workload, frac, threads)
+        m, dt, kind, n = cpu_reference(args.workload, CPU_STRIDE, threads)
         if i >= args.warmup:
             times.append(dt)
             matches = m
     sec = sum(times) / len(times)
     val = matches / sec
-    sample = (f"roots [0, {S}) (1/16 of the edge list) of each of the 36 queries "
-              f"on the 7.8M-edge graph, {threads} threads")
+    sample = cpu_sample_text(CPU_STRIDE, threads, n)
     line = {"metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "int32", "data": "synthetic (seeded generator; public graphs unavailable offline)",
             "impl": "reference",
-            "config": {"workload": f"{args.workload} (root sample)", "sample": sample},
+            "config": workload_config(args.workload),
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": kind,
-                             "sample": sample},
+                             "sample": sample, "host": host_info()},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -352,14 +404,10 @@ def run_gpu_arm(args):
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator with the named shapes; public graphs unavailable offline)",
-        "config": {"workload": "bursty-7.8m-3edge: 1.1M nodes, 7.8M edges, 36 three-edge motifs "
-                               "run separately, delta 86400, count",
-                   "graph_edges": host.num_edges, "graph_vertices": host.num_vertices,
-                   "queries_per_step": len(qs), "matches_per_step": matches,
-                   "l2": "flushed before every step (256 MB write)",
-                   "parallelism": f"replicas x{world}",
-                   "autotune": "per-query, candidates timed on the whole query, outside the timed region"
-                   if tuned else "off"},
+        "config": workload_config(args.workload),
+        "replicas": world,
+        "autotune": "per-query, candidates timed on the whole query, outside the timed region"
+        if tuned else "off",
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e_total / args.steps},
         "gpu_launches": launches,
@@ -375,13 +423,22 @@ def run_gpu_arm(args):
                               "reference semantics, summed over the 36 queries"},
         "clocks": clk.summary(),
     }
+    if rank == 0:
+        line["c1"] = c1_leg(dev, cpu=(world == 1 and not args.no_cpu_baseline))
+    if rank == 0 and world == 1 and not args.no_extra:
+        line["reference_gpu_kernel"] = ref_kernel_leg(host, dg, qs, want, dev)
+        import bench_modes
+        line["enumerate"] = bench_modes.enumerate_leg(warmup=1, steps=3)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        m, sec, kind, S = cpu_reference(args.workload, 0.5, threads)
+        hi = host_info()
+        threads = hi["usable_cores"]
+        m, sec, kind, n = cpu_reference(args.workload, CPU_STRIDE, threads)
+        m1, sec1, _, n1 = cpu_reference(args.workload, CPU_STRIDE_1T, 1)
         line["cpu_baseline"] = {
             "value": m / sec, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"roots [0, {S}) (half the edge list) of each of the 36 queries, "
-                      f"{threads} threads"}
+            "sample": cpu_sample_text(CPU_STRIDE, threads, n), "host": hi,
+            "single_thread": {"value": m1 / sec1, "unit": UNIT,
+                              "sample": cpu_sample_text(CPU_STRIDE_1T, 1, n1)}}
     for w in workers:
         w.close()
     dg.free()
@@ -392,6 +449,116 @@ def run_gpu_arm(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def ref_kernel_leg(host, dg, qs, want, dev) -> dict:
+    """The reference's generated search kernel (KernelGen with its warp
+    options on, built for sm_100a by baseline/refgen.py) on the same 36
+    queries and the same GPU, beside this library's per-query kernel.  Both
+    are timed the reference's way (GPUWorker::timed_run,
+    src/core/cpu/data.cc:534-542): host time around run() with the graph
+    resident, best of two runs per query."""
+    from baseline import refgen as R
+    from everest_b200 import capi
+    if not all(R.available(q["mu"], q["mv"]) for q in qs):
+        return {"available": False, "why": "generated kernels not built (python -m baseline.refgen build)"}
+    rg = R.RefGraph.from_host_graph(host)
+    w = capi.Worker(dev)
+    ref_ms, our_ms = 0.0, 0.0
+    try:
+        for q in qs:
+            c, ms = R.count(rg, q["mu"], q["mv"], q["delta"], reps=2)
+            if c != want[q["name"]]:
+                raise SystemExit(f"reference kernel count mismatch on {q['name']}: {c} != {want[q['name']]}")
+            ref_ms += min(ms)
+            best = None
+            for _ in range(2):
+                w.take(dg, q["mu"], q["mv"], q["delta"])
+                t0 = time.perf_counter()
+                c2 = w.run()
+                dt = (time.perf_counter() - t0) * 1e3
+                best = dt if best is None else min(best, dt)
+            if c2 != want[q["name"]]:
+                raise SystemExit(f"count mismatch on {q['name']}")
+            our_ms += best
+    finally:
+        w.close()
+        rg.free()
+    return {"available": True, "kernel": "reference KernelGen output (warpCentric, warpBalancing, "
+                                         "tailExpansion on) for sm_100a",
+            "queries": len(qs), "reference_ms": ref_ms, "this_library_ms": our_ms,
+            "speedup": ref_ms / max(our_ms, 1e-9), "counts_equal": True,
+            "timing": "host ms around run() per query, graph resident, best of 2; default launch parameters"}
+
+
+def c1_leg(dev, cpu: bool) -> dict:
+    """The CPU-runnable case: 10k nodes / 200k edges (Zipf 1.5), triangle
+    0->1->2->0, delta 3600, count.  GPU: device time with the graph resident
+    (best of 10 after 3 warm-up runs) and end to end from pinned host arrays
+    (upload, build, query, count read back).  CPU: the reference's Baseline
+    body over every root, all host cores and one thread."""
+    import torch
+    from everest_b200 import capi, synth
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        tri = json.load(f)["full_zipf"]["triangle"]
+    spec = synth.SPECS["zipf-10k-200k"]
+    u, v, t = synth.load_or_generate(spec.name)
+    host = capi.graph_build_host(u, v, t, name=spec.name).pin()
+    stream = torch.cuda.Stream(device=dev)
+    sh = stream.cuda_stream
+    dg = capi.DeviceGraph(host, dev, sh)
+    w = capi.Worker(dev, sh)
+    dev_ms = []
+    for i in range(13):
+        w.take(dg, tri["mu"], tri["mv"], tri["delta"])
+        c = w.run()
+        if c != tri["count"]:
+            raise SystemExit(f"200k triangle count {c} != {tri['count']}")
+        if i >= 3:
+            dev_ms.append(w.last_stats()["device_ms"])
+    e2e_ms = []
+    for i in range(8):
+        with torch.cuda.stream(stream):
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            g2 = capi.DeviceGraph(host, dev, sh)
+            w.take(g2, tri["mu"], tri["mv"], tri["delta"])
+            w.launch()
+            c = w.result()
+            ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        g2.free()
+        if c != tri["count"]:
+            raise SystemExit("200k triangle end-to-end count mismatch")
+        if i >= 3:
+            e2e_ms.append(ev0.elapsed_time(ev1))
+    w.close()
+    dg.free()
+    host.unpin()
+    gms, ems = min(dev_ms), statistics.median(e2e_ms)
+    out = {"workload": "zipf-10k-200k: 10k nodes, 200k edges, triangle 0->1->2->0, delta 3600, count",
+           "count": c, "gpu_device_ms": gms, "gpu_e2e_ms": ems,
+           "gpu_matches_per_s": c / (gms / 1e3), "gpu_e2e_matches_per_s": c / (ems / 1e3)}
+    if cpu:
+        from oracle import oracle as O
+        g = O.Graph(u, v, t, spec.num_nodes)
+        if O.ref_lib() is not None:
+            hi = host_info()
+            res = {}
+            for th in (hi["usable_cores"], 1):
+                best = None
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    cc = O.ref_baseline_count(g, tri["mu"], tri["mv"], tri["delta"], threads=th)
+                    dt = time.perf_counter() - t0
+                    best = dt if best is None else min(best, dt)
+                if cc != tri["count"]:
+                    raise SystemExit("200k triangle CPU count mismatch")
+                res[th] = best
+            out["cpu_reference"] = {"kind": "reference", "sample": "every root", "threads": hi["usable_cores"],
+                                    "ms": res[hi["usable_cores"]] * 1e3, "ms_1_thread": res[1] * 1e3,
+                                    "matches_per_s": c / res[hi["usable_cores"]]}
+    return out
 
 
 def run_single_query(args):

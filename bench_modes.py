@@ -131,13 +131,24 @@ def run_batch(args) -> int:
     return 0
 
 
-def run_serve(args) -> int:
+def serve_leg(n: int = 10_000, window: int = 100_000, limit: int = int(1e8), warmup: int = 1, steps: int = 3,
+              slots: str = "64,2,2,2,1.0,2,2") -> dict:
+    """Serving: a stream of n 3-5-edge count and enumerate queries on two
+    resident graphs (7.8M and 63M edges; ``workloads.serve_queries``)
+    through ``serve.Server``, against the same queries one at a time through
+    the plain per-query kernel, every result exact in both (checked).
+
+    The one-at-a-time arm runs each query alone with no work limit; its
+    service times give its capacity and, under the Poisson arrival times
+    below, the latency of a FIFO server.  The served arm keeps queries past
+    ``limit`` adjacency records out of the shared batches and re-runs them
+    on heavy slots (no limit, a fraction of the SMs beside other work).
+    Reported: queries/s with every query submitted at once (the median of
+    ``steps`` passes after ``warmup``), and p50 / p99 / p99.9 latency under
+    Poisson arrivals at 0.8x the one-at-a-time capacity, beside FIFO's."""
     import torch
     from everest_b200 import capi, serve, synth, workloads
     torch.cuda.set_device(0)
-    window = args.window or 100_000
-    n = args.queries or 2000
-    limit = int(args.limit)
     qs = workloads.serve_queries(window, n)
     hosts = {}
     for key in ("bursty-1.1m-7.8m", "bursty-6m-63m"):
@@ -145,8 +156,8 @@ def run_serve(args) -> int:
         u, v, t = synth.load_or_generate(sp.name)
         hosts[sp.name] = capi.graph_build_host(u, v, t, name=sp.name)
     dgs = {k: capi.DeviceGraph(h, 0) for k, h in hosts.items()}
-    _one_at_a_time(capi, dgs, qs[: min(64, n)], limit)  # warm-up
-    seq, svc = _one_at_a_time(capi, dgs, qs, limit)
+    _one_at_a_time(capi, dgs, qs[: min(64, n)], 0)  # warm-up
+    seq, svc = _one_at_a_time(capi, dgs, qs, 0)
     for g in dgs.values():
         g.free()
     seq_total = float(svc.sum())
@@ -161,18 +172,17 @@ def run_serve(args) -> int:
         fin[i] = prev
     seq_lat = fin - arr
     out = {}
-    slots = [float(x) for x in getattr(args, "serve_slots", "64,2,2,2").split(",")]
-    slots += [64, 2, 2, 2, 1.0][len(slots):]
-    mb, ib, es, ebps = (int(x) for x in slots[:4])
-    share = slots[4]
-    # untimed warm-up passes first (the device memory pool grows to its
-    # working size on the first pass), then the timed saturated passes
-    runs = ([("warmup", None)] * max(0, args.warmup) + [("saturated", None)] * max(1, args.steps)
-            + [("poisson", arr)])
+    sl = [float(x) for x in slots.split(",")]
+    sl += [64, 2, 2, 2, 1.0, 2, 2][len(sl):]
+    mb, ib, es, ebps = (int(x) for x in sl[:4])
+    share = sl[4]
+    hs, hbps = int(sl[5]), int(sl[6])
+    runs = [("warmup", None)] * max(0, warmup) + [("saturated", None)] * max(1, steps) + [("poisson", arr)]
     sat_runs = []
     for label, times in runs:
         srv = serve.Server(0, max_batch=mb, inflight_batches=ib, enum_slots=es, limit=limit,
-                           enum_blocks_per_sm=ebps, batch_share=share)
+                           enum_blocks_per_sm=ebps, batch_share=share, heavy_slots=hs,
+                           heavy_blocks_per_sm=hbps)
         for k, h in hosts.items():
             srv.add_graph(k, h)
         futs = []
@@ -190,53 +200,74 @@ def run_serve(args) -> int:
         if bad:
             raise SystemExit(f"served results differ from one-at-a-time results for queries {bad[:8]}")
         st = srv.stats()
+        st["unanswered"] = sum(1 for r in got if r.count is None)
         if label == "saturated":
             sat_runs.append(st)
         elif label == "poisson":
             out[label] = st
         srv.close()
-    # the saturated run is repeated (--steps times): the median run by
-    # queries/s is reported, with every run's queries/s beside it
     sat_runs.sort(key=lambda x: x["queries_per_s"])
     out["saturated"] = dict(sat_runs[len(sat_runs) // 2])
     out["saturated"]["runs_queries_per_s"] = [round(x["queries_per_s"], 1) for x in sat_runs]
     cnt = [i for i, q in enumerate(qs) if not q["cap"]]
-    line = {"metric": "served queries/s and p50/p99/p99.9 latency vs one at a time, exact",
-            "value": out["saturated"]["queries_per_s"], "unit": "queries/s", "n_gpus": 1, "steps": len(sat_runs),
-            "warmup": max(0, args.warmup), "ms_per_step": 1e3 * n / max(out["saturated"]["queries_per_s"], 1e-9),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic (seeded generator)", "mode": "serve",
-            "config": {"workload": f"bursty 7.8M + 63M edges resident; {n} queries, 3-5-edge patterns on 2-4 "
-                                   "nodes, delta log-uniform [600, 604800], 20% enumerate (cap log-uniform "
-                                   f"[1e4, 1e6]), roots = a random window of {window} edges per query",
-                       "work_limit": limit, "poisson_rate_qps": rate,
-                       "max_batch": mb, "batches_in_flight": ib, "enumeration_slots": es,
-                       "enumeration_blocks_per_sm": ebps, "batch_share": share},
-            "one_at_a_time": {"value": seq_qps, "unit": "queries/s",
-                              "service_s": {"count": float(sum(svc[i] for i in cnt)),
-                                            "enumerate": float(sum(svc[i] for i, q in enumerate(qs) if q["cap"])),
-                                            "limited": float(sum(svc[i] for i, r in enumerate(seq) if r[1]))},
-                              "service_p50_ms": _pct(svc, 50), "service_p99_ms": _pct(svc, 99),
-                              "longest_ms": sorted(([int(i), round(float(svc[i]) * 1e3, 2), len(qs[i]["mu"]),
-                                                     qs[i]["cap"], bool(seq[i][1])] for i in range(n)),
-                                                   key=lambda x: -x[1])[:5],
-                              "poisson_p50_ms": _pct(seq_lat, 50), "poisson_p99_ms": _pct(seq_lat, 99),
-                              "poisson_p999_ms": _pct(seq_lat, 99.9)},
-            "served_saturated": out["saturated"], "served_poisson_0.8x": out["poisson"],
-            "speedup": out["saturated"]["queries_per_s"] / seq_qps,
-            "count_queries": len(cnt), "enumerate_queries": n - len(cnt),
-            "limited_queries": int(sum(lim for _, lim, _ in seq)), "results_equal": True}
+    return {
+        "metric": "served queries/s and p50/p99/p99.9 latency vs one at a time, exact",
+        "value": out["saturated"]["queries_per_s"], "unit": "queries/s",
+        "config": {"workload": f"bursty 7.8M + 63M edges resident; {n} queries, 3-5-edge patterns on 2-4 "
+                               "nodes, delta log-uniform [600, 604800], 20% enumerate (cap log-uniform "
+                               f"[1e4, 1e6]), roots = a random window of {window} edges per query",
+                   "batch_work_limit": limit, "poisson_rate_qps": rate,
+                   "max_batch": mb, "batches_in_flight": ib, "enumeration_slots": es,
+                   "enumeration_blocks_per_sm": ebps, "batch_share": share, "heavy_slots": hs,
+                   "heavy_blocks_per_sm": hbps, "warmup": warmup, "steps": steps},
+        "one_at_a_time": {"value": seq_qps, "unit": "queries/s", "work_limit": None,
+                          "service_s": {"count": float(sum(svc[i] for i in cnt)),
+                                        "enumerate": float(sum(svc[i] for i, q in enumerate(qs) if q["cap"]))},
+                          "service_p50_ms": _pct(svc, 50), "service_p99_ms": _pct(svc, 99),
+                          "longest_ms": sorted(([int(i), round(float(svc[i]) * 1e3, 2), len(qs[i]["mu"]),
+                                                 qs[i]["cap"]] for i in range(n)), key=lambda x: -x[1])[:5],
+                          "poisson_p50_ms": _pct(seq_lat, 50), "poisson_p99_ms": _pct(seq_lat, 99),
+                          "poisson_p999_ms": _pct(seq_lat, 99.9)},
+        "served_saturated": out["saturated"], "served_poisson_0.8x": out["poisson"],
+        "speedup": out["saturated"]["queries_per_s"] / seq_qps,
+        "p99_vs_fifo": out["poisson"]["p99_ms"] / max(_pct(seq_lat, 99), 1e-9),
+        "count_queries": len(cnt), "enumerate_queries": n - len(cnt),
+        "requeued_queries": out["saturated"]["requeued"],
+        "limited_unanswered": out["saturated"]["unanswered"] + out["poisson"]["unanswered"],
+        "results_equal": True}
+
+
+def run_serve(args) -> int:
+    """``bench.py --mode serve``: serve_leg as its own JSON line."""
+    leg = serve_leg(n=args.queries or 10_000, window=args.window or 100_000, limit=int(args.limit),
+                    warmup=args.warmup, steps=args.steps, slots=getattr(args, "serve_slots", "64,2,2,2,1.0,2,2"))
+    line = {"metric": leg["metric"], "value": leg["value"], "unit": "queries/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * (args.queries or 10_000) / max(leg["value"], 1e-9), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)",
+            "mode": "serve"}
+    line.update({k: v for k, v in leg.items() if k not in ("metric", "value", "unit")})
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_enumerate(args) -> int:
+def full_size_counts() -> dict:
+    """Counts at full size from the reference's generated kernel on a B200
+    (tests/golden/full_size_counts.json, written by
+    tests/golden/make_full_size_counts.py)."""
+    p = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "full_size_counts.json")
+    with open(p) as f:
+        return json.load(f)
+
+
+def enumerate_leg(warmup: int = 3, steps: int = 5) -> dict:
     """Enumeration under memory admission: the 4-cycle 0->1->2->3->0 on the
     2.6M-node / 36M-edge graph, delta 86400, cap 1e6.  The row buffer
     (cap x 4 int32) is admitted against free device memory by the worker.
-    Reported: rows/s of the capped enumeration, the exact total count and
-    its time, and a host check that every returned row is a distinct valid
-    match (edge order, window, endpoints, injectivity)."""
+    Reported: rows/s of the capped enumeration, the exact total count (equal
+    to the reference's generated kernel's) and its time, and a host check
+    that every returned row is a distinct valid match (edge order, window,
+    endpoints, injectivity)."""
     import torch
     from everest_b200 import capi, synth
     torch.cuda.set_device(0)
@@ -247,19 +278,22 @@ def run_enumerate(args) -> int:
     w = capi.Worker(0)
     count_ms, enum_ms = [], []
     total = rows = None
-    for rep in range(args.warmup + args.steps):
+    for rep in range(warmup + steps):
         w.take(dg, mu, mv, delta)
         total = w.run()
         cm = w.last_stats()["device_ms"]
         w.take(dg, mu, mv, delta, 0, -1, cap)
-        c = w.run()
+        w.run()
         em = w.last_stats()["device_ms"]
         rows = w.enum_rows(cap)
-        if rep >= args.warmup:
+        if rep >= warmup:
             count_ms.append(cm)
             enum_ms.append(em)
     w.close()
     dg.free()
+    want = full_size_counts()["bursty-2.6m-36m"]["4-cycle delta 86400"]
+    if total != want:
+        raise SystemExit(f"4-cycle total {total} != the reference kernel's {want}")
     # host validation of the rows (line ids = sorted edge ids for this graph)
     r = rows.astype(np.int64)
     ok = (r[:, 0] < r[:, 1]) & (r[:, 1] < r[:, 2]) & (r[:, 2] < r[:, 3])
@@ -274,15 +308,23 @@ def run_enumerate(args) -> int:
     if not (ok.all() and distinct and n_rows == expect_rows):
         raise SystemExit("enumeration rows failed the host check")
     em = float(np.median(enum_ms))
-    line = {"metric": "enumerated rows/s under memory admission (capped), exact total beside it",
-            "value": n_rows / (em / 1e3), "unit": "rows/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": em, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)", "mode": "enumerate",
+    return {"metric": "enumerated rows/s under memory admission (capped), exact total beside it",
+            "value": n_rows / (em / 1e3), "unit": "rows/s", "ms": em, "steps": steps, "warmup": warmup,
             "config": {"workload": "bursty 2.6M nodes / 36M edges; 4-cycle 0->1->2->3->0, delta 86400, "
                                    "enumerate cap 1e6 (int32 rows of original line ids)",
                        "row_buffer_bytes": cap * 4 * 4},
-            "rows": n_rows, "exact_total": int(total), "count_ms": float(np.median(count_ms)),
-            "rows_valid_distinct": True}
+            "rows": n_rows, "exact_total": int(total), "exact_total_equals_reference_kernel": True,
+            "count_ms": float(np.median(count_ms)), "rows_valid_distinct": True}
+
+
+def run_enumerate(args) -> int:
+    """``bench.py --mode enumerate``: enumerate_leg as its own JSON line."""
+    leg = enumerate_leg(args.warmup, args.steps)
+    line = {"metric": leg["metric"], "value": leg["value"], "unit": "rows/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": leg["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator)", "mode": "enumerate",
+            "config": leg["config"], "rows": leg["rows"], "exact_total": leg["exact_total"],
+            "count_ms": leg["count_ms"], "rows_valid_distinct": True}
     print(json.dumps(line), flush=True)
     return 0
 

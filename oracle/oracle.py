@@ -109,6 +109,10 @@ def ref_lib():
                                          ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_ulonglong)]
         L.ref_baseline_count.restype = ctypes.c_int
+        if hasattr(L, "ref_baseline_count_strided"):
+            L.ref_baseline_count_strided.argtypes = L.ref_baseline_count.argtypes[:12] + [ctypes.c_int] + \
+                L.ref_baseline_count.argtypes[12:]
+            L.ref_baseline_count_strided.restype = ctypes.c_int
         _ref = L
     return _ref
 
@@ -228,21 +232,31 @@ def enumerate_rows(g: Graph, mu, mv, delta: int, cap: int, roots=None, strict_ts
     return rows[:n].copy(), int(tot.value)
 
 
-def ref_baseline_count(g: Graph, mu, mv, delta: int, roots=None, threads: int = 1):
-    """Count with the host build of the reference's own Baseline body.
-    Raises RuntimeError when that build is absent."""
+def ref_baseline_count(g: Graph, mu, mv, delta: int, roots=None, threads: int = 1, stride: int = 1):
+    """Count with the host build of the reference's own Baseline body over
+    roots rb, rb + stride, ... below re_ (roots = (rb, re_), default every
+    root).  Raises RuntimeError when that build is absent."""
     L = ref_lib()
     if L is None:
         raise RuntimeError("reference Baseline host build not present")
     k = len(mu)
     rb, re_ = roots if roots is not None else default_roots(g, k)
-    eg = np.stack([g.u, g.v, g.t], axis=1).astype(np.int32).ravel()
+    eg = getattr(g, "_eg_aos", None)
+    if eg is None:
+        eg = g._eg_aos = np.stack([g.u, g.v, g.t], axis=1).astype(np.int32).ravel()
     em = np.stack([np.asarray(mu, np.int32), np.asarray(mv, np.int32),
                    np.arange(1, k + 1, dtype=np.int32)], axis=1).ravel()
     out = ctypes.c_ulonglong(0)
-    rc = L.ref_baseline_count(eg, g.E, g.in_eid, g.in_off, g.out_eid, g.out_off, em, k,
-                              motif_nodes(mu, mv), int(delta), int(rb), int(re_),
-                              int(threads), ctypes.byref(out))
+    if stride != 1:
+        if not hasattr(L, "ref_baseline_count_strided"):
+            raise RuntimeError("reference Baseline host build predates root sampling; rebuild it")
+        rc = L.ref_baseline_count_strided(eg, g.E, g.in_eid, g.in_off, g.out_eid, g.out_off, em, k,
+                                          motif_nodes(mu, mv), int(delta), int(rb), int(re_), int(stride),
+                                          int(threads), ctypes.byref(out))
+    else:
+        rc = L.ref_baseline_count(eg, g.E, g.in_eid, g.in_off, g.out_eid, g.out_off, em, k,
+                                  motif_nodes(mu, mv), int(delta), int(rb), int(re_),
+                                  int(threads), ctypes.byref(out))
     if rc != 0:
         raise ValueError("motif too large for the Baseline body (<=5 nodes, <=6 edges)")
     return int(out.value)

@@ -111,12 +111,22 @@ def test_generated_kernel_36_three_edge_motifs():
         assert c == want[name]
 
 
+def _fixture():
+    with open(os.path.join(HERE, "golden", "full_size_counts.json")) as f:
+        return json.load(f)["bursty-2.6m-36m"]
+
+
 def test_generated_kernel_4cycle_36m():
     q = {"name": "4-cycle", "mu": [0, 1, 2, 3], "mv": [1, 2, 3, 0], "delta": 86400}
-    _full_size("bursty-2.6m-36m", [q], "4-cycle, 36M edges, delta 86400")
+    rows = _full_size("bursty-2.6m-36m", [q], "4-cycle, 36M edges, delta 86400")
+    assert rows[0][1] == _fixture()["4-cycle delta 86400"]
 
 
 def test_generated_kernel_batch_mix_slice():
     qs = workloads.refgen_batch_slice()
     assert len(qs) == 16
-    _full_size("bursty-2.6m-36m", qs, "16 queries of the 64-query batch mix, 36M edges")
+    rows = _full_size("bursty-2.6m-36m", qs, "16 queries of the 64-query batch mix, 36M edges")
+    fix = _fixture().get("batch slice")
+    if fix is not None:
+        for name, c, _, _ in rows:
+            assert c == fix[name]["count"], name
