@@ -290,7 +290,8 @@ def query_sets() -> Dict[str, List[dict]]:
                        for mu, mv in sorted(golden) for R_key in [query_key(mu, mv)]],
             "bursty-7.8m-3edge": workloads.queries("bursty-7.8m-3edge"),
             "c3": [dict(q, name=f"c3-{i:02d}") for i, q in enumerate(c3)],
-            "c4-cycle": [{"name": "4-cycle", "mu": [0, 1, 2, 3], "mv": [1, 2, 3, 0], "delta": 86400}]}
+            "c4-cycle": [{"name": "4-cycle", "mu": [0, 1, 2, 3], "mv": [1, 2, 3, 0], "delta": 86400}],
+            "serve-slice": workloads.refgen_serve_slice()}
     return sets
 
 

@@ -61,8 +61,9 @@ extern "C" int refgen_graph_upload(const int *eg_aos, int num_edges, const int *
     gpuErrchk(cudaMemcpy(g->eg, eg_aos, sizeof(corelib::TemporalEdge) * (size_t)num_edges, cudaMemcpyHostToDevice));
     gpuErrchk(cudaMemcpy(g->in_v, in_v, sizeof(int) * (size_t)num_edges, cudaMemcpyHostToDevice));
     gpuErrchk(cudaMemcpy(g->out_v, out_v, sizeof(int) * (size_t)num_edges, cudaMemcpyHostToDevice));
-    gpuErrchk(cudaMemcpy(g->in_r, in_r, sizeof(int) * nv, cudaMemcpyHostToDevice));
-    gpuErrchk(cudaMemcpy(g->out_r, out_r, sizeof(int) * nv, cudaMemcpyHostToDevice));
+    const size_t nr = (size_t)num_vertices + 1;  // the host offsets end here; the padding stays zero
+    gpuErrchk(cudaMemcpy(g->in_r, in_r, sizeof(int) * nr, cudaMemcpyHostToDevice));
+    gpuErrchk(cudaMemcpy(g->out_r, out_r, sizeof(int) * nr, cudaMemcpyHostToDevice));
   } catch (const refgen_error &x) {
     put_error(err, errlen, x.what());
     cudaFree(g->eg); cudaFree(g->in_v); cudaFree(g->out_v); cudaFree(g->in_r); cudaFree(g->out_r);

@@ -208,6 +208,8 @@ int evx_device_count(int *count) {
 static int alloc_graph(int device, int64_t E, int64_t V, evx_graph **out, cudaStream_t s) {
   if (!out) return fail(EVX_ERR_INVALID, "null output pointer");
   if (E < 0 || V < 0) return fail(EVX_ERR_INVALID, "negative sizes");
+  // fewer than 2^30 edges: adjacency records keep positions in 30 bits
+  // (kPosMask) beside two flag bits
   if (E >= INT_MAX / 2 || V >= INT_MAX - 1)
     return fail(EVX_ERR_OVERFLOW, "graph too large for int32 edge / vertex ids");
   int ndev = 0;

@@ -13,7 +13,7 @@ namespace evx {
 //   edges[e]    = {u, v, t, position of e in out_rec}     root fetch
 //   inpos[e]    = position of e in in_rec
 //   euid[e]     = original line id of e                    enumeration rows
-//   out_rec[p]  = {eid, v, t, position of eid in in_rec (low 31 bits; see kPosMask)}   grouped by u, ascending eid
+//   out_rec[p]  = {eid, v, t, position of eid in in_rec (low bits; see kPosMask)}   grouped by u, ascending eid
 //   in_rec[p]   = {eid, u, t, position of eid in out_rec}  grouped by v, ascending eid
 //   node_rng[x] = {out_beg, out_end, in_beg, in_end}       positions in out_rec / in_rec
 //   pair_rec[i] = {eid, t} grouped by static edge (u, v), ascending eid
@@ -59,9 +59,12 @@ __host__ __device__ inline unsigned long long pair_hash(unsigned long long x) {
 }
 
 // The fourth word of an out_rec / in_rec record: the edge's position in its
-// other list in the low 31 bits; the top bit is set when the edge's pair run
-// (same endpoints, same direction) has a later entry.
-constexpr int kPosMask = 0x7fffffff;
+// other list in the low 30 bits; the top bit is set when the edge's pair run
+// (same endpoints, same direction) has a later entry, and bit 30 when its
+// reverse pair's run has an entry after it (graphs hold fewer than 2^30
+// edges, alloc_graph in evx_capi.cu, so positions fit in 30 bits).
+constexpr int kPosMask = 0x3fffffff;
+constexpr int kRevLater = 0x40000000;
 
 // Bit of a node in the 64-bit neighbour signatures (Fibonacci hashing; a
 // different hash from the pair table's).

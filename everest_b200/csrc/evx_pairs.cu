@@ -102,13 +102,20 @@ __global__ void cross_pos_kernel(const int4 *__restrict__ edges, const int4 *__r
 }
 
 // Mark each adjacency record whose edge is followed by another entry of its
-// pair run (top bit of the record's fourth word).
+// pair run (top bit of the record's fourth word) and whose reverse pair has
+// an entry after it (kRevLater).
 __global__ void mark_runs_kernel(int4 *__restrict__ out_rec, int4 *__restrict__ in_rec,
-                                 const int2 *__restrict__ loc, int n) {
+                                 const int2 *__restrict__ loc, const int2 *__restrict__ rev, int n) {
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    const int2 lo = loc[out_rec[p].x], li = loc[in_rec[p].x];
-    if (lo.x + 1 < lo.y) out_rec[p].w |= (int)0x80000000u;
-    if (li.x + 1 < li.y) in_rec[p].w |= (int)0x80000000u;
+    const int eo = out_rec[p].x, ei = in_rec[p].x;
+    const int2 lo = loc[eo], li = loc[ei];
+    int fo = lo.x + 1 < lo.y ? (int)0x80000000u : 0;
+    int fi = li.x + 1 < li.y ? (int)0x80000000u : 0;
+    const int2 ro = rev[eo], ri = rev[ei];
+    if (ro.x < ro.y) fo |= kRevLater;
+    if (ri.x < ri.y) fi |= kRevLater;
+    out_rec[p].w |= fo;
+    in_rec[p].w |= fi;
   }
 }
 
@@ -290,7 +297,7 @@ int build_pair_index(DeviceGraph &g, cudaStream_t s) {
     g.pair_max_probe = h[0];
     rev_loc_kernel<<<grid, block, 0, s>>>(g.view(), g.rev_loc, n);
     cross_pos_kernel<<<grid, block, 0, s>>>(g.edges, g.node_rng, g.out_rec, g.in_rec, g.cross_out, g.cross_in, n);
-    mark_runs_kernel<<<grid, block, 0, s>>>(g.out_rec, g.in_rec, g.pair_loc, n);
+    mark_runs_kernel<<<grid, block, 0, s>>>(g.out_rec, g.in_rec, g.pair_loc, g.rev_loc, n);
     EVX_CUDA(cudaGetLastError());
   }
 cleanup:

@@ -766,7 +766,7 @@ struct Searcher {
             for (int q = 0; q < kScanWide; q++) {
               if (pos + q < end && rw[q].z <= tl) {
                 rw[q].w = __ldg(g.inpos + rw[q].x);
-                pf[q] = __ldg(&g.edges[rw[q].x].w) & kPosMask;
+                pf[q] = __ldg(&g.edges[rw[q].x].w);  // edges[] positions carry no flags
               }
             }
           }
@@ -793,12 +793,14 @@ struct Searcher {
             // them): count the entries of that edge's own pair run (or of the
             // reverse pair's run) after the edge and inside the window
             const bool rev = (qf & kQRevPair) != 0;
-            // (a same-pair candidate whose record says its run ends with it
-            // adds nothing: skip its lookup)
+            // a candidate whose record says its own pair's run (top bit) or
+            // its reverse pair's run (kRevLater) has no entry after it adds
+            // nothing: skip its lookup
             int2 pl[kScanWide];
+            const int later = rev ? kRevLater : (int)0x80000000u;
 #pragma unroll
             for (int q = 0; q < kScanWide; q++) {
-              if (!rev && !prun && rw[q].w >= 0) ok[q] = false;
+              if (!prun && !(rw[q].w & later)) ok[q] = false;
               pl[q] = ok[q] ? __ldg((rev ? g.rev_loc : g.pair_loc) + rw[q].x) : make_int2(0, 0);
             }
 #pragma unroll

@@ -98,6 +98,19 @@ def serve_queries(window: int = 100_000, n: int = 10_000) -> List[dict]:
     return mixed_queries(n, 5, (3, 5), (2, 4), graphs, window, delta_range=(600, 604800), enum_frac=0.2)
 
 
+# 16 count queries of the serving stream (3-, 4- and 5-edge patterns on both
+# graphs, over their 100k-root windows) whose search is cheap (under 2 ms
+# each for this library on a B200).
+SERVE_SLICE = (4, 5, 7, 11, 24, 3, 13, 14, 17, 18, 1, 6, 8, 10, 12, 16)
+
+
+def refgen_serve_slice() -> List[dict]:
+    """SERVE_SLICE of the serving stream: the slice the reference's
+    generated kernel checks."""
+    qs = serve_queries(100_000, 10_000)
+    return [dict(qs[i], name=f"serve-{i:04d}") for i in SERVE_SLICE]
+
+
 CONSTRAINED_DELTA = 86400
 
 

@@ -122,6 +122,14 @@ def test_generated_kernel_4cycle_36m():
     assert rows[0][1] == _fixture()["4-cycle delta 86400"]
 
 
+def test_generated_kernel_serve_slice():
+    """16 count queries of the serving stream on both resident graphs."""
+    qs = workloads.refgen_serve_slice()
+    assert len(qs) == 16 and all(q["cap"] == 0 for q in qs)
+    for gname in sorted({q["graph"] for q in qs}):
+        _full_size(gname, [q for q in qs if q["graph"] == gname], f"serving-stream slice on {gname}")
+
+
 def test_generated_kernel_batch_mix_slice():
     qs = workloads.refgen_batch_slice()
     assert len(qs) == 16
