@@ -67,14 +67,16 @@ def parse():
                          "reference's node / temporal / anti-edge / filter query shapes on the 7.8M graph")
     ap.add_argument("--queries", type=int, default=0, help="batch/serve: number of queries")
     ap.add_argument("--window", type=int, default=0,
-                    help="batch/serve: roots per query (a random time window of the edge list)")
+                    help="batch/serve: roots per query (a random time window of the edge list); batch: "
+                         "0 = every root of the graph (default)")
     ap.add_argument("--serve-slots", default="64,2,2,2,1.0,2,2",
                     help="serve: max queries per batch, batches in flight, enumeration slots, "
                          "blocks per SM of an enumeration (0 = all), share of a batch kernel's blocks, "
                          "heavy slots, blocks per SM of a heavy query beside other work")
-    ap.add_argument("--limit", type=float, default=1e8,
-                    help="batch/serve: work limit per query, in adjacency records examined inside "
-                         "their time windows (stopped queries are flagged in both arms)")
+    ap.add_argument("--limit", type=float, default=None,
+                    help="work limit per query, in adjacency records examined inside their time windows. "
+                         "batch (default 0 = none, every result exact): stopped queries are flagged in both "
+                         "arms; serve (default 1e8): queries past it leave the shared batches for heavy slots")
     return ap.parse_args()
 
 
@@ -429,6 +431,7 @@ def run_gpu_arm(args):
         line["reference_gpu_kernel"] = ref_kernel_leg(host, dg, qs, want, dev)
         import bench_modes
         line["enumerate"] = bench_modes.enumerate_leg(warmup=1, steps=3)
+        line["batch"] = bench_modes.batch_leg(window=0, n=64, limit=0, warmup=1, steps=1)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         hi = host_info()
         threads = hi["usable_cores"]

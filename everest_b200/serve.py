@@ -17,10 +17,13 @@ The reference answers one query at a time and re-uploads the graph for each
 * an optional work limit keeps heavy queries out of the shared batches
   (work = adjacency records examined inside their time windows, fixed by
   the graph and the query): a query past it is stopped on the device and
-  re-queued for a heavy slot, a worker that runs one query at a time with no
-  limit on a fraction of the SMs while other work is about, so that it
-  overlaps the batches instead of holding them back.  Its result is exact
-  like every other (``Result.requeued`` says it took that route).  With
+  re-queued for the heavy slots: workers that run it with no limit, one
+  root range (chunk) at a time -- each chunk launched on a fraction of the
+  SMs while other work is about and on the whole GPU otherwise, so that it
+  overlaps the batches instead of holding them back, and several slots can
+  share one heavy query's chunks.  Its result (the sum over its chunks; an
+  enumeration or a constrained query runs as one chunk) is exact like
+  every other (``Result.requeued`` says it took that route).  With
   ``heavy_slots=0`` a query past the limit is resolved with
   ``Result.limited`` set and no count instead.
 
@@ -57,6 +60,18 @@ class Request:
 
 
 @dataclass
+class HeavyJob:
+    """A query re-run on the heavy slots, root range by root range."""
+    req: Request
+    next_root: int
+    end_root: int
+    chunk: int
+    acc: int = 0
+    inflight: int = 0
+    rows: Optional[np.ndarray] = None
+
+
+@dataclass
 class Result:
     count: Optional[int]
     rows: Optional[np.ndarray] = None
@@ -70,7 +85,7 @@ class Server:
                  enum_slots: int = 2, mem_reserve: int = 1 << 30, idle_sleep_s: float = 50e-6,
                  backend=None, limit: int = 0, use_graph: bool = False, tile_roots: int = 64,
                  enum_blocks_per_sm: int = 2, batch_share: float = 1.0, heavy_slots: int = 2,
-                 heavy_blocks_per_sm: int = 2):
+                 heavy_blocks_per_sm: int = 2, heavy_chunks: int = 32):
         # backend: the module providing Batch, Worker, DeviceGraph and
         # device_mem_info (the C-ABI binding; tests substitute a fake)
         self.be = backend if backend is not None else capi
@@ -114,9 +129,11 @@ class Server:
         self.enum_blocks_per_sm = int(enum_blocks_per_sm)
         self.enum_reqs: List[Optional[Request]] = [None] * enum_slots
         # heavy slots: queries that passed the work limit, re-run without it
-        self.heavy_q: "collections.deque[Request]" = collections.deque()
+        self.heavy_q: "collections.deque[HeavyJob]" = collections.deque()
         self.heavy_workers = [capi_.Worker(device) for _ in range(heavy_slots if self.limit else 0)]
-        self.heavy_reqs: List[Optional[Request]] = [None] * len(self.heavy_workers)
+        # per slot: (job, first root, end root) of the chunk it runs
+        self.heavy_reqs: List[Optional[tuple]] = [None] * len(self.heavy_workers)
+        self.heavy_chunks = max(1, int(heavy_chunks))
         self.heavy_t0: List[float] = [0.0] * len(self.heavy_workers)
         self.heavy_blocks_per_sm = int(heavy_blocks_per_sm)
         self.requeued = 0
@@ -211,10 +228,28 @@ class Server:
                     or any(self.heavy_reqs))
 
     def _requeue(self, reqs: List[Request]) -> None:
-        """Queries past the work limit: run them again on a heavy slot (the
-        caller holds the lock)."""
+        """Queries past the work limit: run them again on the heavy slots
+        (the caller holds the lock).  A count query is cut into about
+        heavy_chunks root ranges; an enumeration (its cap spans every root)
+        or a constrained query runs as one."""
         self.requeued += len(reqs)
-        self.heavy_q.extend(reqs)
+        for r in reqs:
+            g = self.graphs[r.graph]
+            E = getattr(g, "num_edges", None)
+            beg = max(0, r.beg)
+            if E is None:
+                end = r.end
+                chunk = 0  # unknown graph size: one chunk, the request's own range
+            else:
+                top = max(0, int(E) - len(r.mu) + 1)
+                end = top if r.end < 0 else min(r.end, int(E))
+                if end <= beg:  # no roots: nothing to re-run
+                    self._finish(r, Result(0, np.zeros((0, len(r.mu)), np.int32) if r.enum_cap > 0 else None,
+                                           requeued=True))
+                    continue
+                one = r.enum_cap > 0 or r.constraints is not None
+                chunk = (end - beg) if one else -(-(end - beg) // self.heavy_chunks)
+            self.heavy_q.append(HeavyJob(r, beg, end, chunk))
 
     def _finish(self, r: Request, res: Result) -> None:
         now = time.perf_counter()
@@ -259,13 +294,21 @@ class Server:
                     self._finish(r, Result(c, rows, limited=lim))
                 progressed = True
         for i, w in enumerate(self.heavy_workers):
-            r = self.heavy_reqs[i]
-            if r is not None and w.done():
+            slot = self.heavy_reqs[i]
+            if slot is not None and w.done():
+                job = slot[0]
+                r = job.req
                 self.launch_log.append(("heavy", self.heavy_t0[i], time.perf_counter(), 1))
-                c = w.result()
-                rows = w.enum_rows(r.enum_cap) if r.enum_cap > 0 else None
-                self.heavy_reqs[i] = None
-                self._finish(r, Result(c, rows, requeued=True))
+                job.acc += w.result()
+                if r.enum_cap > 0:
+                    job.rows = w.enum_rows(r.enum_cap)
+                with self.lock:
+                    job.inflight -= 1
+                    done = job.inflight == 0 and job.next_root >= job.end_root and \
+                        (not self.heavy_q or self.heavy_q[0] is not job)
+                    self.heavy_reqs[i] = None
+                if done:
+                    self._finish(r, Result(job.acc, job.rows, requeued=True))
                 progressed = True
         return progressed
 
@@ -329,28 +372,38 @@ class Server:
             w.launch()
             self.enum_t0[i] = time.perf_counter()
             progressed = True
-        # heavy queries: one per slot, no work limit, on a fraction of the SMs
-        # while other work is queued or running (the whole GPU otherwise)
+        # heavy queries: chunk by chunk, no work limit, on a fraction of the
+        # SMs while other work is queued or running (the whole GPU otherwise)
         for i, w in enumerate(self.heavy_workers):
             if self.heavy_reqs[i] is not None:
                 continue
             with self.lock:
                 if not self.heavy_q:
                     break
-                r = self.heavy_q[0]
+                job = self.heavy_q[0]
+                r = job.req
             if r.enum_cap > 0:
                 need = r.enum_cap * len(r.mu) * 4
                 free, _ = self.be.device_mem_info(self.device)
                 if need + self.mem_reserve > free:
                     break
             with self.lock:
-                self.heavy_q.popleft()
-                self.heavy_reqs[i] = r
+                if job.chunk <= 0:
+                    b0, b1 = r.beg, r.end  # the request's own range, as submitted
+                    job.next_root = job.end_root
+                else:
+                    b0 = job.next_root
+                    b1 = min(job.end_root, b0 + job.chunk)
+                    job.next_root = b1
+                job.inflight += 1
+                if job.next_root >= job.end_root:
+                    self.heavy_q.popleft()  # every chunk handed out
+                self.heavy_reqs[i] = (job, b0, b1)
             if r.constraints is not None:
-                w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags,
+                w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, b0, b1, r.enum_cap, r.flags,
                        constraints=r.constraints)
             else:
-                w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, r.beg, r.end, r.enum_cap, r.flags)
+                w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, b0, b1, r.enum_cap, r.flags)
             if hasattr(w, "set_tuning"):
                 busy = bool(self.count_q or self.enum_q) or any(x is not None for x in self.batch_reqs) \
                     or any(x is not None for x in self.enum_reqs)
@@ -381,7 +434,7 @@ class Server:
                 pending = list(self.count_q) + list(self.enum_q)
                 pending += [r for reqs in self.batch_reqs if reqs for r in reqs]
                 pending += [r for r in self.enum_reqs if r]
-                pending += list(self.heavy_q) + [r for r in self.heavy_reqs if r]
+                pending += [j.req for j in self.heavy_q] + [s[0].req for s in self.heavy_reqs if s]
             for r in pending:
                 if not r.future.done():
                     r.future.set_exception(e)

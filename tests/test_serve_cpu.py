@@ -215,6 +215,33 @@ def test_root_ranges_and_count_limit(graph):
     srv.close()
 
 
+class _SizedName(str):
+    """A graph handle of the fake backend that knows its edge count (the
+    server cuts heavy queries into root ranges with it)."""
+
+
+def test_heavy_query_runs_in_root_chunks(graph):
+    be = FakeBackend({"g": graph}, free_bytes=1 << 40)
+    sized = _SizedName("g")
+    sized.num_edges = graph.u.size
+    be.DeviceGraph = lambda host, device: sized
+    mu, mv, d = [0, 1, 2], [1, 2, 0], 3000
+    exact = O.count(graph, mu, mv, d)[0]
+    small = O.count(graph, [0, 1], [1, 0], 400)[0]
+    srv = serve.Server(max_batch=4, inflight_batches=1, enum_slots=1, mem_reserve=0, backend=be,
+                       limit=max(small, 1), heavy_slots=2, heavy_chunks=5)
+    srv.add_graph("g", "g")
+    f_heavy = srv.submit("g", mu, mv, d)
+    f_small = srv.submit("g", [0, 1], [1, 0], 400)
+    srv.drain(60)
+    r = f_heavy.result(1)
+    assert r.requeued and not r.limited and r.count == exact
+    assert f_small.result(1).count == small and not f_small.result(1).requeued
+    assert sum(1 for k, *_ in srv.launch_log if k == "heavy") == 5  # five root ranges
+    assert srv.stats()["requeued"] == 1
+    srv.close()
+
+
 def test_enumerations_share_the_gpu_only_beside_count_work(graph):
     # enumerations launched while count queries are queued or running take
     # the configured fraction of the SMs; alone they take the whole GPU (0)
