@@ -76,7 +76,7 @@ int enqueue(evx_batch *b, int nq) {
     const int tiles = b->groups[gi + 3], grid = b->groups[gi + 4];
     const bool ps = b->groups[gi + 5] != 0;
     if (tiles <= 0) continue;
-    LaunchArgs la;
+    LaunchArgs la{};
     la.table = b->table_d + beg;
     la.nq = n;
     la.total_tiles = tiles;

@@ -519,8 +519,8 @@ int evx_worker_take_constrained(evx_worker *w, const evx_graph *gh, int k, const
     return evx_worker_take(w, gh, k, mu, mv, delta, beg, end, enum_cap, flags);
   if (!w || !gh || !mu || !mv) return fail(EVX_ERR_INVALID, "null argument");
   if (gh->g.device != w->device) return fail(EVX_ERR_INVALID, "graph and worker on different devices");
-  if (flags & ~EVX_FLAG_EXACT_TOTAL)
-    return fail(EVX_ERR_INVALID, "constrained searches take no flag but EVX_FLAG_EXACT_TOTAL");
+  if (flags & ~(EVX_FLAG_EXACT_TOTAL | EVX_FLAG_PER_LANE))
+    return fail(EVX_ERR_INVALID, "constrained searches take no flag but EVX_FLAG_EXACT_TOTAL and EVX_FLAG_PER_LANE");
   MotifPlan plan;
   int rc = build_plan(k, mu, mv, &plan);
   if (rc) return rc;
@@ -596,6 +596,27 @@ int evx_worker_take_constrained(evx_worker *w, const evx_graph *gh, int k, const
   rc = cons_build_masks(*c, plan.n, g.node_feat, (int)V, g.edge_feat, (int)E, w->node_ok_d, w->edge_ok_d,
                         w->num_sms, w->stream);
   if (rc) return rc;
+  if (c->anti_mask == 0 && !c->has_filter && !(flags & EVX_FLAG_PER_LANE)) {
+    // node / edge predicates and temporal gaps only: the warp-synchronous
+    // search with the checks compiled in (the CS kernels).  Range
+    // arithmetic counts edges without looking at them, so it stays only
+    // where no counted edge has a check: closing last edges under node
+    // predicates alone.
+    rc = evx_worker_take(w, gh, k, mu, mv, delta, beg, end, enum_cap, flags & EVX_FLAG_EXACT_TOTAL);
+    if (rc) return rc;
+    SearchArgs &a = w->args;
+    a.limit = 0;  // no work limit on constrained jobs
+    a.cons.node_ok = c->node_mode ? w->node_ok_d : nullptr;
+    a.cons.edge_ok = c->has_edge ? w->edge_ok_d : nullptr;
+    a.cons.has_gap = c->has_temporal ? 1 : 0;
+    for (int j = 0; j < k - 1; j++) a.cons.gap[j] = cs.temporal[j];
+    // (with gaps, a closing edge's window starts from the edge before it,
+    // so the closing-endpoint check made with the level's own window is off)
+    int tf = kQPairScan | (c->has_temporal ? kQNoPrune : 0);
+    if (!c->has_edge && !c->has_temporal) tf |= tail_mode(plan, 0, enum_cap > 0) & ~kQNewArith;
+    a.tail_flags = tf;
+    return EVX_OK;
+  }
   cs.plan = plan;
   cs.root_beg = (int)beg;
   cs.root_end = (int)end;
@@ -671,8 +692,9 @@ int evx_worker_launch(evx_worker *w) {
   int bps = w->blocks_per_sm;
   if (bps <= 0) {
     const int qf = (a.strict_ts ? kQStrict : 0) | a.tail_flags;
-    int rc = search_occupancy(w->plan.k, a.enumerate != 0, plan_pair_scan(w->plan, qf, a.enumerate != 0),
-                              w->block, &bps);
+    const bool cs = cons_any(a.cons);
+    int rc = search_occupancy(w->plan.k, a.enumerate != 0, cs || plan_pair_scan(w->plan, qf, a.enumerate != 0),
+                              cs, w->block, &bps);
     if (rc) return rc;
     if (bps <= 0) bps = 1;
   }

@@ -143,6 +143,16 @@ struct EnumArgs {
 };
 
 // A search launch: nq queries sharing one work queue of root tiles.
+// Node / edge predicates and temporal gaps of a constrained single query run
+// by the warp-synchronous search (no anti-edge, no filter; those take the
+// per-lane constrained kernel).  All null / zero for a plain query.
+struct ConsArgs {
+  const unsigned short *node_ok;  // [V] bit a: the node may be motif node a (null: all)
+  const unsigned char *edge_ok;   // [E] edge predicate (null: all)
+  int has_gap;                    // motif edge j (j >= 1) ends its window at
+  int gap[EVX_MAX_MOTIF_EDGES];   // [j-1]: t(e_{j-1}) + gap, not after t(e_0) + delta (j >= 2)
+};
+
 struct LaunchArgs {
   const QueryDesc *table;     // device table (nq > 1); ignored when nq == 1
   int nq;
@@ -154,6 +164,7 @@ struct LaunchArgs {
                               // meter passes it is stopped early
   unsigned long long *meter;  // [nq] matches + queued partial matches per query
                               // (maintained only when limit > 0)
+  ConsArgs cons;              // single constrained query (the CS kernels); zero otherwise
 };
 
 // Search job arguments (one query).
@@ -174,6 +185,7 @@ struct SearchArgs {
   int *stop;                  // [1] set when the enumeration cap is reached
   unsigned long long limit;   // work limit (0 = none), count mode only
   unsigned long long *meter;  // [1] matches + queued partial matches (limit > 0)
+  ConsArgs cons;              // node / edge predicates and temporal gaps (zero: none)
 };
 
 // Host-side graph object.
@@ -247,8 +259,10 @@ int table_occupancy(int k, bool ps, int *blocks_per_sm);
 // kernels are compiled with and without that walk).
 bool plan_pair_scan(const MotifPlan &plan, int qflags, bool enumerate);
 // Max resident blocks per SM for a given motif size / mode / pair-run
-// variant / block.
-int search_occupancy(int k, bool enumerate, bool ps, int block, int *blocks_per_sm);
+// variant / constrained variant (cs) / block.
+int search_occupancy(int k, bool enumerate, bool ps, bool cs, int block, int *blocks_per_sm);
+// Whether search args carry constraints (the CS kernel variant runs them).
+inline bool cons_any(const ConsArgs &c) { return c.node_ok || c.edge_ok || c.has_gap; }
 
 // A constrained search (evx_constrained.cu).  prev_real[j] = the latest motif
 // edge before j that is not an anti-edge (0 for j = 1).

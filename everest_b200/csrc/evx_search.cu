@@ -48,7 +48,7 @@ constexpr int kBlock = 128;     // threads per block
 constexpr int kWarps = kBlock / 32;
 // Records each lane loads per round in a non-last level's scan.
 #ifndef EVX_SCAN_WIDE
-#define EVX_SCAN_WIDE 2
+#define EVX_SCAN_WIDE 4
 #endif
 constexpr int kScanWide = EVX_SCAN_WIDE;
 
@@ -63,7 +63,7 @@ constexpr int kScanWide = EVX_SCAN_WIDE;
 #define EVX_MINB3 8
 #endif
 #ifndef EVX_MINB4
-#define EVX_MINB4 6
+#define EVX_MINB4 8
 #endif
 constexpr int min_blocks(int k) { return k <= 3 ? EVX_MINB3 : (k == 4 ? EVX_MINB4 : 4); }
 
@@ -238,7 +238,7 @@ struct Prev {
   int eid, t, src, dst, pop, pip;
 };
 
-template <int K, bool ENUM, bool EXACT, bool PS>
+template <int K, bool ENUM, bool EXACT, bool PS, bool CS>
 struct Searcher {
   static constexpr int L = K - 1;          // levels; level l opens motif edge l + 1
   static constexpr int N = K + 1;          // motif nodes <= k + 1
@@ -347,6 +347,19 @@ struct Searcher {
     return p.dst == x ? p.pip + 1 : (p.src == x ? __ldg(g.cross_in + p.eid) : -1);
   }
 
+  // Constrained queries (CS): a candidate also needs its edge predicate and,
+  // when it maps a new motif node (want < 0), that node's predicate (bit nmc
+  // of its mask: the new node's index is the number mapped before it).
+  __device__ __forceinline__ bool cons_ok(int eid, int node, int want, int nmc) const {
+    if constexpr (!CS) {
+      return true;
+    } else {
+      if (la.cons.edge_ok && !__ldg(la.cons.edge_ok + eid)) return false;
+      if (want < 0 && la.cons.node_ok && !((__ldg(la.cons.node_ok + node) >> nmc) & 1)) return false;
+      return true;
+    }
+  }
+
   __device__ __forceinline__ bool structural_ok(int node, int want, int nmc, const int (&m)[N]) const {
     if (want >= 0) return node == want;
     bool ok = true;
@@ -426,6 +439,12 @@ struct Searcher {
       }
     }
     int tl = sm.root[root].z;
+    if constexpr (CS) {
+      // temporal gaps: motif edge l + 1 ends its window gap[l] after the
+      // previous edge (edge 1: after the root, even past delta; later ones
+      // never past t(e_0) + delta)
+      if (la.cons.has_gap && has) tl = l == 0 ? p.t + la.cons.gap[0] : min(p.t + la.cons.gap[l], tl);
+    }
 
     // ---------------------------- last level through the pair hash table ----
     if (!ENUM && (qf & kQPairHash) && l == kr() - 2) {
@@ -538,9 +557,18 @@ struct Searcher {
     if (l == kr() - 2 || l == L - 1) {
       // ------------------------------------------------ last level ----
       bool arith = true;  // the range-arithmetic check is still to be made
+      int chk = 0;
       while (true) {
         const unsigned act = __ballot_sync(kFull, pos < end);
         if (!act) break;
+        if (la.limit && ((++chk) & 63) == 0 && halted()) {
+          // a long scan with a work limit: the query passed it; stop here
+          pos = end;
+          __syncwarp();
+          if (lane == 0) sm.halt = 1;
+          __syncwarp();
+          break;
+        }
         if (act != kFull && si && ((++steps) & (si - 1)) == 0)
           rebalance(act, pos, end, want, out, prun, base, slot, root, tl, m, e);
         bool emit = false;
@@ -567,7 +595,7 @@ struct Searcher {
                 pos = end;
               } else {
                 ++cand;
-                if (structural_ok(rr[q].y, want, nmc, m)) {
+                if (structural_ok(rr[q].y, want, nmc, m) && cons_ok(rr[q].x, rr[q].y, want, nmc)) {
                   ++cnt;
                   if (ENUM) { emit = true; last_eid = rr[q].x; }
                 }
@@ -677,7 +705,7 @@ struct Searcher {
         }
         if (lo >= hi || ld_t(lst + lo) > tl) {
           pos = end;
-        } else if (EVX_REVERSE_CLOSE && !ENUM && !strict_() && !(qf & (kQSamePair | kQRevPair))) {
+        } else if (EVX_REVERSE_CLOSE && !ENUM && !CS && !strict_() && !(qf & (kQSamePair | kQRevPair))) {
           // Few closing edges: count the task from the closing side.  Each
           // closing edge e2 (x, c) inside the window pairs with the
           // candidates e1 of this level that map the same new node c and
@@ -685,27 +713,27 @@ struct Searcher {
           // pair (base, c) (or (c, base)) with edge id in (p, e2).  Taken
           // when the window holds at most kRevMax closing edges and more
           // candidates than that.
-          int4 c3[kRevMax];
+          // (the window's times first, then each closing record again when
+          // it is used: fewer registers live than holding all records)
+          int t3[kRevMax];
 #pragma unroll
-          for (int j = 0; j < kRevMax; j++) c3[j] = (lo + j < hi) ? __ldg(lst + lo + j) : make_int4(0, 0, INT_MAX, 0);
+          for (int j = 0; j < kRevMax; j++) t3[j] = (lo + j < hi) ? ld_t(lst + lo + j) : INT_MAX;
           const bool more = lo + kRevMax < hi && ld_t(lst + lo + kRevMax) <= tl;
           int n2 = 0;
 #pragma unroll
-          for (int j = 0; j < kRevMax; j++) n2 += c3[j].z <= tl ? 1 : 0;
+          for (int j = 0; j < kRevMax; j++) n2 += t3[j] <= tl ? 1 : 0;
           const int4 *lst1 = out ? g.out_rec : g.in_rec;
           if (!more && pos + n2 < end && ld_t(lst1 + pos + n2) <= tl) {
+            for (int j = 0; j < n2; j++) {
+              const int4 c3 = __ldg(lst + lo + j);
+              const int cn = c3.y;
+              bool fresh = true;
 #pragma unroll
-            for (int j = 0; j < kRevMax; j++) {
-              if (j < n2) {
-                const int cn = c3[j].y;
-                bool fresh = true;
-#pragma unroll
-                for (int q = 0; q < N; q++) fresh = fresh && !(q < nmc && m[q] == cn);
-                const int a_ = out ? base : cn, b_ = out ? cn : base;
-                if (fresh && pair_maybe(g, a_, b_)) {
-                  const int2 f = pair_find(g, a_, b_);
-                  cnt += (unsigned long long)pair_count_eids(g, f.x, f.y, p.eid + 1, c3[j].x - 1);
-                }
+              for (int q = 0; q < N; q++) fresh = fresh && !(q < nmc && m[q] == cn);
+              const int a_ = out ? base : cn, b_ = out ? cn : base;
+              if (fresh && pair_maybe(g, a_, b_)) {
+                const int2 f = pair_find(g, a_, b_);
+                cnt += (unsigned long long)pair_count_eids(g, f.x, f.y, p.eid + 1, c3.x - 1);
               }
             }
             cand += (unsigned)(n2 + 1);
@@ -713,6 +741,7 @@ struct Searcher {
           }
         }
       }
+      int chk = 0;
       while (true) {
         const unsigned act = __ballot_sync(kFull, pos < end);
         if (!inline_here) {
@@ -736,6 +765,15 @@ struct Searcher {
           }
         }
         if (!act) break;
+        if (this->la.limit && ((++chk) & 63) == 0 && halted()) {  // (la here: the last edge's a)
+          // a long scan with a work limit: the query passed it; drop its
+          // queued tasks and unwind (its result is discarded)
+          pos = end;
+          __syncwarp();
+          if (lane == 0) { sm.halt = 1; sm.nb[l + 1] = 0; }
+          __syncwarp();
+          break;
+        }
         if (act != kFull && si && ((++steps) & (si - 1)) == 0)
           rebalance(act, pos, end, want, out, prun, base, slot, root, tl, m, e);
         // the next kScanWide records of every lane's range in one round of
@@ -784,7 +822,7 @@ struct Searcher {
                 pos = end;
               } else {
                 ++cand;
-                ok[q] = structural_ok(rw[q].y, want, nmc, m);
+                ok[q] = structural_ok(rw[q].y, want, nmc, m) && cons_ok(rw[q].x, rw[q].y, want, nmc);
               }
             }
           }
@@ -848,7 +886,7 @@ struct Searcher {
                 pos = end;
               } else {
                 ++cand;
-                push = structural_ok(rc.y, want, nmc, m);
+                push = structural_ok(rc.y, want, nmc, m) && cons_ok(rc.x, rc.y, want, nmc);
               }
             }
             push_children<l>(push, slot, rc, out, base, pf[q], root);
@@ -929,7 +967,7 @@ struct Searcher {
 // Persistent search: warps claim root tiles from one work queue covering
 // every query of the launch, switch their per-warp query copy when a tile
 // belongs to another query, and add each query's count to counts[q].
-template <int K, bool ENUM, bool EXACT, bool PS>
+template <int K, bool ENUM, bool EXACT, bool PS, bool CS>
 __global__ void __launch_bounds__(kBlock, min_blocks(K))
 search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const LaunchArgs la,
               const __grid_constant__ EnumArgs ea) {
@@ -940,7 +978,7 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
   if (lane < K) sm.nb[lane] = 0;
   if (lane == 0) { sm.halt = 0; sm.cur_q = 0; }
   __syncwarp();
-  Searcher<K, ENUM, EXACT, PS> S(g, sm.q.plan, ea, la, sm, lane);
+  Searcher<K, ENUM, EXACT, PS, CS> S(g, sm.q.plan, ea, la, sm, lane);
   int cur_q = -1;
   auto flush = [&]() {
     if (cur_q >= 0) {
@@ -1003,7 +1041,14 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
       bool has = false;
       if (r < re) {
         const int4 ed = __ldg(g.edges + r);
-        if (ed.x != ed.y) {  // self-loops are not roots
+        bool ok = ed.x != ed.y;  // self-loops are not roots
+        if constexpr (CS) {
+          // the root is motif edge 0 = 0 -> 1: its edge and both node predicates
+          if (ok && la.cons.edge_ok) ok = __ldg(la.cons.edge_ok + r) != 0;
+          if (ok && la.cons.node_ok)
+            ok = ((__ldg(la.cons.node_ok + ed.x) & 1) != 0) && ((__ldg(la.cons.node_ok + ed.y) & 2) != 0);
+        }
+        if (ok) {
           sm.root[lane] = make_int4(ed.x, ed.y, ed.z + delta, r);
           has = true;
         }
@@ -1039,7 +1084,7 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
 
 // The shared-memory attribute belongs to the function on the current
 // device, so it is set once per device (bit d of the mask: device d).
-template <int K, bool ENUM, bool EXACT, bool PS>
+template <int K, bool ENUM, bool EXACT, bool PS, bool CS>
 int setup_k() {
   static std::atomic<unsigned long long> done{0ull};
   int dev = 0;
@@ -1047,11 +1092,11 @@ int setup_k() {
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
   const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
   if (bit && (done.load(std::memory_order_acquire) & bit)) return 0;
-  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT, PS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT, PS, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(kWarps * sizeof(WarpSmem<K>)));
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
 #ifdef EVX_CARVEOUT
-  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT, PS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  e = cudaFuncSetAttribute(search_kernel<K, ENUM, EXACT, PS, CS>, cudaFuncAttributePreferredSharedMemoryCarveout,
                            EVX_CARVEOUT);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(carveout)");
 #endif
@@ -1059,20 +1104,20 @@ int setup_k() {
   return 0;
 }
 
-template <int K, bool ENUM, bool EXACT, bool PS>
+template <int K, bool ENUM, bool EXACT, bool PS, bool CS>
 int launch_k(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, const EnumArgs &ea, int grid,
              cudaStream_t s) {
-  int rc = setup_k<K, ENUM, EXACT, PS>();
+  int rc = setup_k<K, ENUM, EXACT, PS, CS>();
   if (rc) return rc;
-  search_kernel<K, ENUM, EXACT, PS><<<grid, kBlock, kWarps * sizeof(WarpSmem<K>), s>>>(g, q0, la, ea);
+  search_kernel<K, ENUM, EXACT, PS, CS><<<grid, kBlock, kWarps * sizeof(WarpSmem<K>), s>>>(g, q0, la, ea);
   return 0;
 }
 
-template <int K, bool ENUM, bool EXACT, bool PS>
+template <int K, bool ENUM, bool EXACT, bool PS, bool CS>
 int occ_k(int *bps) {
-  int rc = setup_k<K, ENUM, EXACT, PS>();
+  int rc = setup_k<K, ENUM, EXACT, PS, CS>();
   if (rc) return rc;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, search_kernel<K, ENUM, EXACT, PS>, kBlock,
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, search_kernel<K, ENUM, EXACT, PS, CS>, kBlock,
                                                                 kWarps * sizeof(WarpSmem<K>));
   return e == cudaSuccess ? 0 : cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
 }
@@ -1097,11 +1142,15 @@ constexpr int kSingleTileRoots = 64;
 }  // namespace
 
 // single-query launches: exact motif size, count or enumerate, with or
-// without the pair-run walk (PS: compiled out where no level needs it)
+// without the pair-run walk (PS: compiled out where no level needs it), and
+// the constrained variant (CS: node / edge predicates and temporal gaps,
+// always with the walk)
 #define EVX_K_CASE(FN, KK, ...)                                                      \
   case KK:                                                                           \
-    if (enumerate) return ps ? FN<KK, true, true, true>(__VA_ARGS__) : FN<KK, true, true, false>(__VA_ARGS__); \
-    return ps ? FN<KK, false, true, true>(__VA_ARGS__) : FN<KK, false, true, false>(__VA_ARGS__);
+    if (cs) return enumerate ? FN<KK, true, true, true, true>(__VA_ARGS__)            \
+                             : FN<KK, false, true, true, true>(__VA_ARGS__);          \
+    if (enumerate) return ps ? FN<KK, true, true, true, false>(__VA_ARGS__) : FN<KK, true, true, false, false>(__VA_ARGS__); \
+    return ps ? FN<KK, false, true, true, false>(__VA_ARGS__) : FN<KK, false, true, false, false>(__VA_ARGS__);
 #define EVX_K_DISPATCH(FN, ...)                                        \
   switch (k) {                                                         \
     EVX_K_CASE(FN, 2, __VA_ARGS__)                                     \
@@ -1133,7 +1182,7 @@ int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &a
   const int k = plan.k;
   const bool enumerate = args.enumerate != 0;
   const QueryDesc q0 = single_query(plan, args);
-  LaunchArgs la;
+  LaunchArgs la{};
   la.table = nullptr;
   la.nq = 1;
   la.tile_roots = kSingleTileRoots;
@@ -1150,24 +1199,26 @@ int launch_search(const GraphView &g, const MotifPlan &plan, const SearchArgs &a
   ea.stop = args.stop;
   ea.count = args.count;
   const bool ps = plan_pair_scan(plan, q0.flags, enumerate);
+  la.cons = args.cons;
+  const bool cs = cons_any(args.cons);
   EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
 }
 
 int launch_table(const GraphView &g, const QueryDesc &q0, const LaunchArgs &la, int k, bool ps, int grid,
                  cudaStream_t stream) {
-  const bool enumerate = false;
+  const bool enumerate = false, cs = false;
   EnumArgs ea;
   memset(&ea, 0, sizeof(ea));
   EVX_K_DISPATCH(launch_k, g, q0, la, ea, grid, stream)
 }
 
-int search_occupancy(int k, bool enumerate, bool ps, int block, int *blocks_per_sm) {
+int search_occupancy(int k, bool enumerate, bool ps, bool cs, int block, int *blocks_per_sm) {
   (void)block;
   EVX_K_DISPATCH(occ_k, blocks_per_sm)
 }
 
 int table_occupancy(int k, bool ps, int *blocks_per_sm) {
-  const bool enumerate = false;
+  const bool enumerate = false, cs = false;
   EVX_K_DISPATCH(occ_k, blocks_per_sm)
 }
 

@@ -91,7 +91,7 @@ int static_query(const DeviceGraph &g, const int *k, const int *mu, const int *m
   a->cursor = reinterpret_cast<int *>(scratch + EVX_STATIC_MAX_QUERIES + q);
   a->stop = a->cursor + 1;
   int bps = 0;
-  rc = search_occupancy(kq, false, plan_pair_scan(*plan, a->tail_flags, false), 128, &bps);
+  rc = search_occupancy(kq, false, plan_pair_scan(*plan, a->tail_flags, false), false, 128, &bps);
   if (rc) return rc;
   if (bps < 1) bps = 1;
   *grid = bps * sms;

@@ -19,9 +19,8 @@ The reference answers one query at a time and re-uploads the graph for each
   the graph and the query): a query past it is stopped on the device and
   re-queued for the heavy slots: workers that run it with no limit, one
   root range (chunk) at a time -- each chunk launched on a fraction of the
-  SMs while other work is about and on the whole GPU otherwise, so that it
-  overlaps the batches instead of holding them back, and several slots can
-  share one heavy query's chunks.  Its result (the sum over its chunks; an
+  SMs (heavy_blocks_per_sm), so that it overlaps the batches instead of
+  holding them back, and several slots share one heavy query's chunks.  Its result (the sum over its chunks; an
   enumeration or a constrained query runs as one chunk) is exact like
   every other (``Result.requeued`` says it took that route).  With
   ``heavy_slots=0`` a query past the limit is resolved with
@@ -85,7 +84,7 @@ class Server:
                  enum_slots: int = 2, mem_reserve: int = 1 << 30, idle_sleep_s: float = 50e-6,
                  backend=None, limit: int = 0, use_graph: bool = False, tile_roots: int = 64,
                  enum_blocks_per_sm: int = 2, batch_share: float = 1.0, heavy_slots: int = 2,
-                 heavy_blocks_per_sm: int = 2, heavy_chunks: int = 32):
+                 heavy_blocks_per_sm: int = 2, heavy_chunks: int = 64):
         # backend: the module providing Batch, Worker, DeviceGraph and
         # device_mem_info (the C-ABI binding; tests substitute a fake)
         self.be = backend if backend is not None else capi
@@ -405,9 +404,10 @@ class Server:
             else:
                 w.take(self.graphs[r.graph], r.mu, r.mv, r.delta, b0, b1, r.enum_cap, r.flags)
             if hasattr(w, "set_tuning"):
-                busy = bool(self.count_q or self.enum_q) or any(x is not None for x in self.batch_reqs) \
-                    or any(x is not None for x in self.enum_reqs)
-                w.set_tuning(block=128, blocks_per_sm=self.heavy_blocks_per_sm if busy else 0,
+                # a heavy chunk never takes the whole GPU: a persistent kernel
+                # holds its blocks until it ends, and light work that arrives
+                # meanwhile would wait behind it
+                w.set_tuning(block=128, blocks_per_sm=self.heavy_blocks_per_sm,
                              roots_per_fetch=32, steal_interval=16, min_split=2)
             w.launch()
             self.heavy_t0[i] = time.perf_counter()

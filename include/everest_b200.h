@@ -65,6 +65,10 @@ extern "C" {
  * This scans the shorter of out(u) / in(v) instead, as the reference does
  * (system/templates/common/resolveMi.snp:9-28). */
 #define EVX_FLAG_LIST_SCAN 256u
+/* evx_worker_take_constrained: run a query with only node / edge predicates
+ * and temporal gaps on the per-lane constrained search (the one anti-edges
+ * and filters take) instead of the warp-synchronous search. */
+#define EVX_FLAG_PER_LANE 512u
 
 typedef struct evx_graph evx_graph;   /* a graph resident on one device */
 typedef struct evx_worker evx_worker; /* per-device search worker */
@@ -345,9 +349,12 @@ EVX_API int evx_graph_set_features(evx_graph *g, const int *node_features, const
  * anti-edge touching a node that no earlier real edge maps, a filter naming
  * an anti-edge, and enumeration with anti-edges (its rows would name no
  * edge); node / edge predicates need the matching features on the graph.
- * Flags: EVX_FLAG_EXACT_TOTAL only.  The plain search's launch, result and
- * rows calls then run this job; the work limit (evx_worker_set_limit) does
- * not apply to it.  A struct with no constraint set runs the plain search. */
+ * Flags: EVX_FLAG_EXACT_TOTAL and EVX_FLAG_PER_LANE only.  A query with
+ * node / edge predicates and temporal gaps only runs on the warp-synchronous
+ * search with the checks compiled in; anti-edges or a filter take the
+ * per-lane constrained search.  The plain search's launch, result and rows
+ * calls then run this job; the work limit (evx_worker_set_limit) does not
+ * apply to it.  A struct with no constraint set runs the plain search. */
 EVX_API int evx_worker_take_constrained(evx_worker *w, const evx_graph *g, int k, const int *mu,
                                         const int *mv, int delta, int64_t beg, int64_t end,
                                         int64_t enum_cap, unsigned flags, const evx_constraints *c);

@@ -56,6 +56,10 @@ def test_reference_generated_counts(worker):
             cons = Constraints.from_yaml(c["constraints"], c["mu"], c["mv"])
             got = run(worker, dg, c["mu"], c["mv"], c["delta"], cons)
             assert got == c["count"], (gname, c["motif"], c["constraints"], got, c["count"])
+            # node / edge / gap-only queries run the warp-synchronous search by
+            # default; the per-lane search gives the same counts
+            got2 = run(worker, dg, c["mu"], c["mv"], c["delta"], cons, flags=capi.FLAG_PER_LANE)
+            assert got2 == c["count"], (gname, c["motif"], c["constraints"], got2, "per lane")
             n += 1
         dg.free()
     assert n == len(cases)
@@ -72,6 +76,12 @@ CONS = [
                                   "edge": "f % 5 != 2", "filter": "e0 + e1 + e2 + e3 > 12"}),
     ([0, 0, 0], [1, 2, 3], {"temporal": [2000, 500], "edge": "(f & 3) != 1"}),
     ([0, 1, 0], [1, 0, 1], {"filter": "e0 * e2 - e1 > 10"}),
+    # warp-synchronous constrained search (no anti-edge, no filter)
+    ([0, 1, 2, 3], [1, 2, 3, 0], {"node0": "f > 3", "node1": "f < 8", "node2": "f > 1", "node3": "f != 5"}),
+    ([0, 1, 2, 3], [1, 2, 3, 0], {"node": "f % 3 != 0", "temporal": [4000, 8000, 3000]}),
+    ([0, 1, 1, 0], [1, 0, 2, 2], {"edge": "f % 4 != 1", "node2": "f > 4", "node0": "f > 0", "node1": "f > 0"}),
+    ([0, 0, 1, 2], [1, 2, 2, 0], {"temporal": [9000, 2000, 2000]}),
+    ([0, 1, 2], [1, 0, 1], {"node": "f > 2"}),
 ]
 
 
@@ -132,6 +142,28 @@ def test_enumeration_rows(worker):
     keep = set(map(tuple, rows_o.tolist()))
     assert len(set(map(tuple, part.tolist()))) == cap and all(tuple(r) in keep for r in part.tolist())
     assert run(worker, dg, mu, mv, 30_000, cons, enum_cap=cap, flags=capi.FLAG_EXACT_TOTAL) == total
+    dg.free()
+
+
+def test_enumeration_rows_warp_synchronous(worker):
+    """Node predicates and temporal gaps only (the warp-synchronous search):
+    rows equal the oracle's, and equal the per-lane search's."""
+    u, v, t = _bursty(100_000, 5_000, 33)
+    rng = np.random.Generator(np.random.PCG64(34))
+    nf = rng.integers(0, 10, 5_000).astype(np.int32)
+    ef = rng.integers(0, 10, u.size).astype(np.int32)
+    g = O.Graph(u, v, t, 5_000)
+    dg = upload(u, v, t, nf, ef)
+    for mu, mv, c in (([0, 1, 2], [1, 2, 0], {"node": "f > 2", "temporal": [20_000, 20_000]}),
+                      ([0, 1, 2, 0], [1, 0, 0, 2], {"edge": "f != 3", "node2": "f < 7", "node0": "f > 0",
+                                                    "node1": "f > 0"})):
+        cons = Constraints.from_yaml(dict(c, delta=30_000), mu, mv)
+        rows_o, total = O.enumerate_constrained(g, mu, mv, 30_000, cons.to_struct(), 10**6, nf, ef)
+        assert 0 < total < 10**6
+        for flags in (0, capi.FLAG_PER_LANE):
+            assert run(worker, dg, mu, mv, 30_000, cons, enum_cap=total + 10, flags=flags) == total
+            rows = worker.enum_rows(total + 10)
+            assert sorted(map(tuple, rows.tolist())) == sorted(map(tuple, rows_o.tolist())), (mu, mv, c, flags)
     dg.free()
 
 
