@@ -13,11 +13,23 @@ before every step); ``e2e`` goes through the public API from pinned host
 arrays: graph upload (host->device + on-device packing), the 36 queries and
 the 36 counts read back, every step.
 
+Beside the headline (N = 1, rank 0), the same line carries:
+  c1                    the 200k-edge triangle on the GPU and on the host;
+  reference_gpu_kernel  the reference's own generated kernel for sm_100a
+                        (baseline/refgen.py) on the same 36 queries;
+  enumerate             the 36M-edge 4-cycle at cap 1e6 (rows checked);
+  batch                 the 64-query mix over the whole 36M-edge graph,
+                        batched vs one at a time, every result exact;
+  serve                 the serving stream (two resident graphs), served vs
+                        one at a time: queries/s, and p50/p99/p99.9 under
+                        Poisson arrivals beside a FIFO server's;
+  cpu_baseline          the reference's Baseline body on the host cores.
+
 ``--impl reference`` times the reference's own CPU implementation of the
 path: its legacy Baseline search body (plugins/GPUWorkerBaseline.cu) built
-for the host (oracle/_ref), on all host cores, over a bounded root sample of
-the same workload.  When that build is absent, the C restatement of the
-same semantics (oracle/) stands in.
+for the host (oracle/_ref), on all host cores, over every 16th root of each
+query of the same workload.  When that build is absent, the C restatement
+of the same semantics (oracle/) stands in.
 
 Multi-GPU: the path does not shard on one-GPU deployments; N ranks run N
 independent replicas (weak scaling), timed as the max over ranks.
@@ -432,6 +444,11 @@ def run_gpu_arm(args):
         import bench_modes
         line["enumerate"] = bench_modes.enumerate_leg(warmup=1, steps=3)
         line["batch"] = bench_modes.batch_leg(window=0, n=64, limit=0, warmup=1, steps=1)
+        # C5's stream shape at 2000 queries over 1000-root windows, so that the
+        # one-at-a-time arm (every query exact) and the Poisson pass stay
+        # within a few minutes: a handful of 5-edge queries at deltas of days
+        # take seconds alone even on such windows
+        line["serve"] = bench_modes.serve_leg(n=2000, window=1000, limit=int(1e8), warmup=0, steps=1)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         hi = host_info()
         threads = hi["usable_cores"]

@@ -33,6 +33,7 @@ FLAG_NO_CLOSING_PRUNE = 64
 FLAG_NEW_SCAN = 128
 FLAG_LIST_SCAN = 256
 FLAG_PER_LANE = 512
+FLAG_WARP_SYNC = 1024
 MAX_MOTIF_EDGES = 8
 
 # every symbol include/everest_b200.h declares

@@ -48,7 +48,7 @@ constexpr int kBlock = 128;     // threads per block
 constexpr int kWarps = kBlock / 32;
 // Records each lane loads per round in a non-last level's scan.
 #ifndef EVX_SCAN_WIDE
-#define EVX_SCAN_WIDE 4
+#define EVX_SCAN_WIDE 2
 #endif
 constexpr int kScanWide = EVX_SCAN_WIDE;
 
@@ -63,7 +63,7 @@ constexpr int kScanWide = EVX_SCAN_WIDE;
 #define EVX_MINB3 8
 #endif
 #ifndef EVX_MINB4
-#define EVX_MINB4 8
+#define EVX_MINB4 7
 #endif
 constexpr int min_blocks(int k) { return k <= 3 ? EVX_MINB3 : (k == 4 ? EVX_MINB4 : 4); }
 
@@ -173,9 +173,14 @@ __device__ __forceinline__ int pair_window(const GraphView &g, int start, int le
 #define EVX_REVERSE_CLOSE 1
 #endif
 #ifndef EVX_REV_MAX
-#define EVX_REV_MAX 8
+#define EVX_REV_MAX 16
+#endif
+// ... and when the task has more than this many candidates per closing edge
+#ifndef EVX_REV_RATIO
+#define EVX_REV_RATIO 1
 #endif
 constexpr int kRevMax = EVX_REV_MAX;  // most closing edges counted that way
+constexpr int kRevRatio = EVX_REV_RATIO;
 
 // A new-node last edge's window is counted by range arithmetic when more than
 // this many records per already-mapped node remain (one pair probe each).
@@ -711,19 +716,15 @@ struct Searcher {
           // candidates e1 of this level that map the same new node c and
           // come between the previous edge and e2, i.e. the entries of the
           // pair (base, c) (or (c, base)) with edge id in (p, e2).  Taken
-          // when the window holds at most kRevMax closing edges and more
-          // candidates than that.
-          // (the window's times first, then each closing record again when
-          // it is used: fewer registers live than holding all records)
-          int t3[kRevMax];
-#pragma unroll
-          for (int j = 0; j < kRevMax; j++) t3[j] = (lo + j < hi) ? ld_t(lst + lo + j) : INT_MAX;
-          const bool more = lo + kRevMax < hi && ld_t(lst + lo + kRevMax) <= tl;
-          int n2 = 0;
-#pragma unroll
-          for (int j = 0; j < kRevMax; j++) n2 += t3[j] <= tl ? 1 : 0;
+          // when the window holds at most kRevMax closing edges and more than
+          // kRevRatio candidates per closing edge.
+          // (the window's closing edges are counted by a gallop bounded at
+          // kRevMax + 1 records; each closing record is loaded when used)
+          const int cap_hi = min(hi, lo + kRevMax + 1);
+          const int n2 = list_first_t_after(lst, lo, cap_hi, tl) - lo;
+          const bool more = n2 > kRevMax;
           const int4 *lst1 = out ? g.out_rec : g.in_rec;
-          if (!more && pos + n2 < end && ld_t(lst1 + pos + n2) <= tl) {
+          if (!more && pos + kRevRatio * n2 < end && ld_t(lst1 + pos + kRevRatio * n2) <= tl) {
             for (int j = 0; j < n2; j++) {
               const int4 c3 = __ldg(lst + lo + j);
               const int cn = c3.y;

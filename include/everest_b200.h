@@ -65,10 +65,13 @@ extern "C" {
  * This scans the shorter of out(u) / in(v) instead, as the reference does
  * (system/templates/common/resolveMi.snp:9-28). */
 #define EVX_FLAG_LIST_SCAN 256u
-/* evx_worker_take_constrained: run a query with only node / edge predicates
- * and temporal gaps on the per-lane constrained search (the one anti-edges
- * and filters take) instead of the warp-synchronous search. */
+/* evx_worker_take_constrained: a query with node predicates alone runs on
+ * the warp-synchronous search, one with an edge predicate or temporal gaps
+ * (and no anti-edge or filter) on the per-lane search.  EVX_FLAG_PER_LANE
+ * sends the first kind to the per-lane search too; EVX_FLAG_WARP_SYNC sends
+ * the second kind to the warp-synchronous search. */
 #define EVX_FLAG_PER_LANE 512u
+#define EVX_FLAG_WARP_SYNC 1024u
 
 typedef struct evx_graph evx_graph;   /* a graph resident on one device */
 typedef struct evx_worker evx_worker; /* per-device search worker */
@@ -349,10 +352,11 @@ EVX_API int evx_graph_set_features(evx_graph *g, const int *node_features, const
  * anti-edge touching a node that no earlier real edge maps, a filter naming
  * an anti-edge, and enumeration with anti-edges (its rows would name no
  * edge); node / edge predicates need the matching features on the graph.
- * Flags: EVX_FLAG_EXACT_TOTAL and EVX_FLAG_PER_LANE only.  A query with
- * node / edge predicates and temporal gaps only runs on the warp-synchronous
+ * Flags: EVX_FLAG_EXACT_TOTAL, EVX_FLAG_PER_LANE and EVX_FLAG_WARP_SYNC
+ * only.  A query with node predicates alone runs on the warp-synchronous
  * search with the checks compiled in; anti-edges or a filter take the
- * per-lane constrained search.  The plain search's launch, result and rows
+ * per-lane constrained search, and so do edge predicates and temporal gaps
+ * unless EVX_FLAG_WARP_SYNC is given.  The plain search's launch, result and rows
  * calls then run this job; the work limit (evx_worker_set_limit) does not
  * apply to it.  A struct with no constraint set runs the plain search. */
 EVX_API int evx_worker_take_constrained(evx_worker *w, const evx_graph *g, int k, const int *mu,

@@ -56,10 +56,13 @@ def test_reference_generated_counts(worker):
             cons = Constraints.from_yaml(c["constraints"], c["mu"], c["mv"])
             got = run(worker, dg, c["mu"], c["mv"], c["delta"], cons)
             assert got == c["count"], (gname, c["motif"], c["constraints"], got, c["count"])
-            # node / edge / gap-only queries run the warp-synchronous search by
-            # default; the per-lane search gives the same counts
+            # both searches give the same counts: node / edge / gap-only
+            # queries on the warp-synchronous one, every query on the per-lane one
             got2 = run(worker, dg, c["mu"], c["mv"], c["delta"], cons, flags=capi.FLAG_PER_LANE)
             assert got2 == c["count"], (gname, c["motif"], c["constraints"], got2, "per lane")
+            if not cons.to_struct().anti_mask and not cons.to_struct().has_filter:
+                got3 = run(worker, dg, c["mu"], c["mv"], c["delta"], cons, flags=capi.FLAG_WARP_SYNC)
+                assert got3 == c["count"], (gname, c["motif"], c["constraints"], got3, "warp sync")
             n += 1
         dg.free()
     assert n == len(cases)
@@ -100,6 +103,8 @@ def test_large_graph_against_oracle(worker):
         want = O.count_constrained(g, mu, mv, delta, cons.to_struct(), nf, ef)
         got = run(worker, dg, mu, mv, delta, cons)
         assert got == want, (mu, mv, c, got, want)
+        if "antiEdge" not in c and "filter" not in c:
+            assert run(worker, dg, mu, mv, delta, cons, flags=capi.FLAG_WARP_SYNC) == want, (mu, mv, c)
         # a sub-range of roots
         want = O.count_constrained(g, mu, mv, delta, cons.to_struct(), nf, ef, roots=(1000, 90_000))
         assert run(worker, dg, mu, mv, delta, cons, beg=1000, end=90_000) == want
@@ -146,8 +151,9 @@ def test_enumeration_rows(worker):
 
 
 def test_enumeration_rows_warp_synchronous(worker):
-    """Node predicates and temporal gaps only (the warp-synchronous search):
-    rows equal the oracle's, and equal the per-lane search's."""
+    """Node / edge predicates and temporal gaps without anti-edges or a
+    filter: rows equal the oracle's on both searches (default routing, the
+    per-lane search, the warp-synchronous search)."""
     u, v, t = _bursty(100_000, 5_000, 33)
     rng = np.random.Generator(np.random.PCG64(34))
     nf = rng.integers(0, 10, 5_000).astype(np.int32)
@@ -160,7 +166,7 @@ def test_enumeration_rows_warp_synchronous(worker):
         cons = Constraints.from_yaml(dict(c, delta=30_000), mu, mv)
         rows_o, total = O.enumerate_constrained(g, mu, mv, 30_000, cons.to_struct(), 10**6, nf, ef)
         assert 0 < total < 10**6
-        for flags in (0, capi.FLAG_PER_LANE):
+        for flags in (0, capi.FLAG_PER_LANE, capi.FLAG_WARP_SYNC):
             assert run(worker, dg, mu, mv, 30_000, cons, enum_cap=total + 10, flags=flags) == total
             rows = worker.enum_rows(total + 10)
             assert sorted(map(tuple, rows.tolist())) == sorted(map(tuple, rows_o.tolist())), (mu, mv, c, flags)
