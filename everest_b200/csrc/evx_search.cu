@@ -26,10 +26,12 @@
 //  * a list opening finds its start in O(1) when the list is the previous
 //    edge's own out/in list (the record carries the edge's position in its
 //    other list), otherwise by a warp-converged binary search;
-//  * when some lanes of a level run dry, idle lanes take equal contiguous
-//    slices of the widest remaining candidate range of that level (one warp
-//    shuffle of the donor's state; an exact partition), in place of the
-//    reference's one-candidate-per-thief split (system/templates/warpBalancing/top.snp)
+//  * when some lanes of a level run dry, idle lanes take interleaved slices
+//    of the widest remaining candidate range of that level -- the donor and
+//    its thieves each take every parts-th record, so they read neighbouring
+//    records in the same step and finish together (one warp shuffle of the
+//    donor's state; an exact partition) -- in place of the reference's
+//    one-candidate-per-thief split (system/templates/warpBalancing/top.snp)
 //    and its host-driven dump/expand rounds (system/templates/tailExpan/Expanding.snp);
 //  * the last level reads several records per lane per step (count mode);
 //  * enumeration slots are reserved with one warp-aggregated atomicAdd per
@@ -51,6 +53,12 @@ constexpr int kWarps = kBlock / 32;
 #define EVX_SCAN_WIDE 2
 #endif
 constexpr int kScanWide = EVX_SCAN_WIDE;
+
+// Rebalancing hands out interleaved slices (a thief takes every parts-th
+// record of the donor's range); 0 hands out contiguous slices instead.
+#ifndef EVX_STRIDED
+#define EVX_STRIDED 1
+#endif
 
 // Check the neighbour signatures before a pair-table lookup.
 #ifndef EVX_PAIR_SIG
@@ -487,6 +495,7 @@ struct Searcher {
     const int kind = plan_kind(w);
     const int nmc = plan_nm(w);
     int pos = 0, end = 0, want = -1, base = 0;
+    int stride = 1;  // distance between this lane's records (interleaved slices)
     bool out = true;
     bool prun = false;  // the range is a run of pair_rec (the edge's static pair), not a list
     int blo = 0, bhi = 0;
@@ -575,27 +584,28 @@ struct Searcher {
           break;
         }
         if (act != kFull && si && ((++steps) & (si - 1)) == 0)
-          rebalance(act, pos, end, want, out, prun, base, slot, root, tl, m, e);
+          rebalance(act, pos, end, stride, want, out, prun, base, slot, root, tl, m, e);
         bool emit = false;
         int last_eid = 0;
+        const int st = EVX_STRIDED ? stride : 1;
         if (pos < end) {
           const int4 *lst = out ? g.out_rec : g.in_rec;
           int4 rr[WIDE];
 #pragma unroll
           for (int q = 0; q < WIDE; q++) {
-            if (q == 0 || pos + q < end) {
+            if (q == 0 || pos + q * st < end) {
               if (prun) {
-                const int2 pr = __ldg(g.pair_rec + pos + q);
+                const int2 pr = __ldg(g.pair_rec + pos + q * st);
                 rr[q] = make_int4(pr.x, want, pr.y, 0);
               } else {
-                rr[q] = __ldg(lst + pos + q);
+                rr[q] = __ldg(lst + pos + q * st);
               }
             }
           }
 #pragma unroll
           for (int q = 0; q < WIDE; q++) {
             if (pos < end) {
-              ++pos;
+              pos += st;
               if (rr[q].z > tl) {
                 pos = end;
               } else {
@@ -608,7 +618,7 @@ struct Searcher {
             }
           }
           if constexpr (!ENUM) {
-            if (want < 0 && pos < end && arith && (qf & kQNewArith)) {
+            if (want < 0 && pos < end && arith && (qf & kQNewArith) && st == 1) {
               // a last edge that maps a new node, and the window goes on past
               // this step: when the rest of the window is long, it counts
               // every record except those whose other endpoint is already
@@ -751,13 +761,17 @@ struct Searcher {
             // park this level's state in shared memory while the warp descends,
             // so none of it stays live in registers across the nested batch
             sm.save[l][lane][0] = make_int4(pos, end, want, base);
-            sm.save[l][lane][1] = make_int4(slot, root, tl, (steps << 2) | (prun ? 2 : 0) | (out ? 1 : 0));
+            // flags word: steps (mod 256, only its low bits matter) | stride (< 2^20) | prun | out
+            sm.save[l][lane][1] = make_int4(slot, root, tl, (int)(((unsigned)steps & 0xffu) << 24) |
+                                                                ((EVX_STRIDED ? stride : 1) << 2) | (prun ? 2 : 0) |
+                                                                (out ? 1 : 0));
             __syncwarp();
             descend<l>();
             const int4 s0 = sm.save[l][lane][0], s1 = sm.save[l][lane][1];
             pos = s0.x; end = s0.y; want = s0.z; base = s0.w;
             slot = s1.x; root = s1.y; tl = s1.z; out = (s1.w & 1) != 0; prun = PS && (s1.w & 2) != 0;
-            steps = s1.w >> 2;
+            steps = (int)((unsigned)s1.w >> 24);
+            stride = EVX_STRIDED ? (s1.w >> 2) & 0x3fffff : 1;
             if (sm.halt) pos = end;  // the query stopped: unwind this level too
             Prev dummy;
             int rr;
@@ -776,7 +790,8 @@ struct Searcher {
           break;
         }
         if (act != kFull && si && ((++steps) & (si - 1)) == 0)
-          rebalance(act, pos, end, want, out, prun, base, slot, root, tl, m, e);
+          rebalance(act, pos, end, stride, want, out, prun, base, slot, root, tl, m, e);
+        const int st = EVX_STRIDED ? stride : 1;
         // the next kScanWide records of every lane's range in one round of
         // loads (one memory latency instead of kScanWide), then processed
         // one at a time; records not processed before a descend are
@@ -790,20 +805,20 @@ struct Searcher {
 #pragma unroll
           for (int q = 0; q < kScanWide; q++) {
             rw[q] = make_int4(0, 0, 0, 0);
-            pf[q] = pos + q;
-            if (pos + q < end) {
+            pf[q] = pos + q * st;
+            if (pos + q * st < end) {
               if (prun) {
-                const int2 pr = __ldg(g.pair_rec + pos + q);
+                const int2 pr = __ldg(g.pair_rec + pos + q * st);
                 rw[q] = make_int4(pr.x, want, pr.y, 0);
               } else {
-                rw[q] = __ldg(lst + pos + q);
+                rw[q] = __ldg(lst + pos + q * st);
               }
             }
           }
           if (prun && !inline_here) {
 #pragma unroll
             for (int q = 0; q < kScanWide; q++) {
-              if (pos + q < end && rw[q].z <= tl) {
+              if (pos + q * st < end && rw[q].z <= tl) {
                 rw[q].w = __ldg(g.inpos + rw[q].x);
                 pf[q] = __ldg(&g.edges[rw[q].x].w);  // edges[] positions carry no flags
               }
@@ -818,7 +833,7 @@ struct Searcher {
           for (int q = 0; q < kScanWide; q++) {
             ok[q] = false;
             if (pos < end) {
-              ++pos;
+              pos += st;
               if (rw[q].z > tl) {
                 pos = end;
               } else {
@@ -882,7 +897,7 @@ struct Searcher {
             bool push = false;
             const int4 rc = rw[q];
             if (pos < end) {
-              ++pos;
+              pos += st;
               if (rc.z > tl) {
                 pos = end;
               } else {
@@ -898,12 +913,14 @@ struct Searcher {
     }
   }
 
-  // Idle lanes take equal slices of the widest remaining range at this level.
+  // Idle lanes take equal slices of the widest remaining range at this level
+  // (contiguous, or interleaved with EVX_STRIDED: every parts-th record).
   template <int NN, int EE>
-  __device__ __forceinline__ void rebalance(unsigned act, int &pos, int &end, int &want, bool &out,
+  __device__ __forceinline__ void rebalance(unsigned act, int &pos, int &end, int &stride, int &want, bool &out,
                                             bool &prun, int &base, int &slot, int &root, int &tl,
                                             int (&m)[NN], int (&e)[EE]) {
-    const int width = end - pos;
+    const int st = EVX_STRIDED ? stride : 1;
+    const int width = EVX_STRIDED ? (end - pos + st - 1) / st : end - pos;
     const unsigned wmax = __reduce_max_sync(kFull, (unsigned)(width > 0 ? width : 0));
     if ((int)wmax < sm.q.min_split) return;
     const int donor = __ffs(__ballot_sync(kFull, (unsigned)width == wmax)) - 1;
@@ -913,6 +930,8 @@ struct Searcher {
     const int parts = nthief + 1;
     const int rank = __popc(idle & lt);
     const bool thief = ((idle >> lane) & 1u) && rank < nthief;
+    const int d_st = EVX_STRIDED ? __shfl_sync(kFull, st, donor) : 1;
+    if (EVX_STRIDED && (long long)d_st * parts >= (1 << 20)) return;  // a stride must fit its 20 bits
     const int p0 = __shfl_sync(kFull, pos, donor);
 #pragma unroll
     for (int q = 0; q < NN; q++) {
@@ -933,6 +952,20 @@ struct Searcher {
     const int d_root = __shfl_sync(kFull, root, donor);
     const int d_tl = __shfl_sync(kFull, tl, donor);
     const int w = (int)wmax;
+    if (EVX_STRIDED) {
+      // interleaved: record i of the donor's remaining range goes to part
+      // i mod parts; all parts keep the donor's end
+      const int d_end = __shfl_sync(kFull, end, donor);
+      if (thief) {
+        want = d_want; out = (d_out & 1) != 0; prun = PS && (d_out & 2) != 0; base = d_base; slot = d_slot;
+        root = d_root; tl = d_tl;
+        pos = p0 + (rank + 1) * d_st;
+        end = d_end;
+        stride = d_st * parts;
+      }
+      if (lane == donor) stride = d_st * parts;
+      return;
+    }
     if (thief) {
       want = d_want; out = (d_out & 1) != 0; prun = PS && (d_out & 2) != 0; base = d_base; slot = d_slot;
       root = d_root; tl = d_tl;

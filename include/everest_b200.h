@@ -343,7 +343,11 @@ typedef struct evx_constraints {
 
 /* Node features (int32 per graph vertex id) and edge features (int32 per
  * sorted edge id) of a resident graph; either may be NULL (kept as before).
- * Host arrays, copied to the graph's device. */
+ * Host arrays, copied to the graph's device on the legacy default stream.
+ * Set them before taking constrained jobs on the graph, not while one is
+ * taken or running: a job's predicate masks are built from the features
+ * when it is taken, and its filter reads the edge features while it runs,
+ * so a change in between would mix old and new values. */
 EVX_API int evx_graph_set_features(evx_graph *g, const int *node_features, const int *edge_features);
 
 /* evx_worker_take with constraints (c may be NULL: plain search).  Checks
