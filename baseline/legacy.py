@@ -71,7 +71,7 @@ def build(force: bool = False) -> List[str]:
     jobs = []
     for name in PLUGINS:
         so = library_path(name)
-        if os.path.exists(so) and not force:
+        if not force and not R.stale(so):
             continue
         with open(os.path.join(ref, "plugins", f"GPUWorker{name}.cu")) as f:
             body = patch(name, f.read())

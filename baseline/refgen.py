@@ -130,6 +130,14 @@ def _nvcc() -> str:
     return cand if os.path.exists(cand) else "nvcc"
 
 
+def stale(so: str) -> bool:
+    """Whether a built library is missing or older than the driver or shim."""
+    if not os.path.exists(so):
+        return True
+    t = os.path.getmtime(so)
+    return any(os.path.getmtime(os.path.join(HERE, f)) > t for f in ("refgen_driver.cu", "refgen_shim.h"))
+
+
 def _compile(body_path: str, so: str) -> str:
     cmd = [_nvcc(), *ARCH, "-O3", "-std=c++17", "-w", "-Xcompiler", "-fPIC", "-shared", "-cudart", "shared",
            "-I", HERE, f'-DREFGEN_BODY="{body_path}"', "-o", so, os.path.join(HERE, "refgen_driver.cu")]
@@ -149,7 +157,7 @@ def build(patterns: Sequence[Tuple[Sequence[int], Sequence[int]]], jobs: int = 0
     todo: Dict[str, Tuple[List[int], List[int]]] = {}
     for mu, mv in patterns:
         key = query_key(mu, mv)
-        if force or not os.path.exists(library_path(mu, mv)):
+        if force or stale(library_path(mu, mv)):
             todo[key] = (list(mu), list(mv))
     if not todo:
         return []
