@@ -71,6 +71,14 @@ def parse():
     ap.add_argument("--single-query", type=int, default=-1,
                     help="profiling aid: run only query I of the workload --reps times and exit")
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--motif", default="",
+                    help="profiling aid: run this motif (edges a-b separated by commas, nodes numbered by first "
+                         "appearance, e.g. 0-1,1-2,2-3,3-0) on the workload's graph --reps times and exit")
+    ap.add_argument("--delta", type=int, default=86400, help="with --motif: the time window")
+    ap.add_argument("--constrained-query", default="",
+                    help="profiling aid: run this constrained bench query (M4-no, M4-v, M4-t, M4-all, M4-f) on "
+                         "the 7.8M-edge graph with its features --reps times and exit")
+    ap.add_argument("--flags", type=int, default=0, help="with --motif / --constrained-query: EVX_FLAG_* bits")
     ap.add_argument("--mode", default="single", choices=["single", "batch", "serve", "enumerate", "constrained"],
                     help="single: the 36-query per-query-kernel step (default); batch: 64 mixed queries "
                          "in one persistent launch per motif size vs the same queries one at a time; serve: "
@@ -582,16 +590,32 @@ def c1_leg(dev, cpu: bool) -> dict:
 
 
 def run_single_query(args):
-    """Run one query of the workload a few times on cuda:0 (for ncu captures)."""
+    """Run one query a few times on cuda:0 (for ncu captures): query I of
+    the workload (--single-query), a motif on the workload's graph
+    (--motif, --delta), or a constrained bench query (--constrained-query)."""
     from everest_b200 import capi, synth, workloads
     stats = workload_stats(args.workload)
     spec = synth.SPECS[stats["graph"]]
-    q = workloads.queries(args.workload)[args.single_query]
     u, v, t = synth.load_or_generate(spec.name)
-    dg = capi.DeviceGraph(capi.graph_build_host(u, v, t), 0)
+    host = capi.graph_build_host(u, v, t)
+    dg = capi.DeviceGraph(host, 0)
+    cons = None
+    if args.constrained_query:
+        from everest_b200.constraints import Constraints
+        byname = {name: (mu, mv, c) for name, mu, mv, c in workloads.constrained_queries()}
+        mu, mv, c = byname[args.constrained_query]
+        nf, ef = workloads.constrained_features(int(max(u.max(), v.max())) + 1, u.size)
+        dg.set_features(nf[host.original_vertex_ids(u, v)], ef)
+        q = {"name": args.constrained_query, "mu": mu, "mv": mv, "delta": c["delta"]}
+        cons = Constraints.from_yaml(c, mu, mv)
+    elif args.motif:
+        pairs = [tuple(int(x) for x in e.split("-")) for e in args.motif.split(",")]
+        q = {"name": args.motif, "mu": [a for a, b in pairs], "mv": [b for a, b in pairs], "delta": args.delta}
+    else:
+        q = workloads.queries(args.workload)[args.single_query]
     w = capi.Worker(0)
     for _ in range(args.reps):
-        w.take(dg, q["mu"], q["mv"], q["delta"])
+        w.take(dg, q["mu"], q["mv"], q["delta"], 0, -1, 0, args.flags, constraints=cons)
         c = w.run()
         print(json.dumps({"query": q["name"], "count": c, **w.last_stats()}), flush=True)
     w.close()
@@ -601,7 +625,7 @@ def run_single_query(args):
 
 def main():
     args = parse()
-    if args.single_query >= 0:
+    if args.single_query >= 0 or args.motif or args.constrained_query:
         return run_single_query(args)
     if args.mode in ("batch", "serve", "enumerate", "constrained"):
         import bench_modes
