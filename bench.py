@@ -15,6 +15,8 @@ the 36 counts read back, every step.
 
 Beside the headline (N = 1, rank 0), the same line carries:
   c1                    the 200k-edge triangle on the GPU and on the host;
+  four_cycle            the 4-cycle on the bench graph: kernel time and its
+                        effective rate against the measured HBM bandwidth;
   reference_gpu_kernel  the reference's own generated kernel for sm_100a
                         (baseline/refgen.py) on the same 36 queries;
   enumerate             the 36M-edge 4-cycle at cap 1e6 (rows checked);
@@ -116,14 +118,15 @@ def measured_peaks():
 
 
 def profile_traffic():
-    """Per-launch DRAM bytes of the search kernel from the committed ncu
-    summary (a line 'traffic_bytes_per_launch: N'), or None."""
+    """DRAM bytes (read + write) of the search kernel over one timed step
+    (its 36 launches, the unit `roofline.achieved` is computed on) from the
+    committed ncu summary (a line 'traffic_bytes_per_step: N'), or None."""
     p = os.path.join(ROOT, "profiles", "search_kernel_bursty-7.8m.md")
     if not os.path.exists(p):
         return None
     with open(p) as f:
         for line in f:
-            if line.strip().startswith("traffic_bytes_per_launch:"):
+            if line.strip().startswith("traffic_bytes_per_step:"):
                 try:
                     return float(line.split(":", 1)[1].strip().split()[0])
                 except ValueError:
@@ -376,7 +379,11 @@ def run_gpu_arm(args):
     step_ms, kern_ms, launches = [], [], 0
     with ClockSampler(dev) as clk:
         for _ in range(args.steps):
+            # an NVTX range per timed step, so that ncu can capture exactly
+            # its launches (--nvtx --nvtx-include timed_step/)
+            torch.cuda.nvtx.range_push("timed_step")
             ms, counts, kms, nl = device_step()
+            torch.cuda.nvtx.range_pop()
             per_query_ms = {q["name"]: round(w.last_stats()["device_ms"], 3) for q, w in zip(qs, workers)}
             step_ms.append(ms)
             kern_ms.append(kms)
@@ -440,6 +447,8 @@ def run_gpu_arm(args):
         "edges_visited_per_s": world * cands / (ms_per_step / 1e3),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
+                     "traffic_unit": "DRAM bytes read + written by the search kernel over one step "
+                                     "(36 launches), from one ncu capture of the timed step",
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "model": "bytes_alg = 12 roots + 8 r_reads + 16 candidates of the serial "
                               "reference semantics, summed over the 36 queries"},
@@ -448,6 +457,7 @@ def run_gpu_arm(args):
     if rank == 0:
         line["c1"] = c1_leg(dev, cpu=(world == 1 and not args.no_cpu_baseline))
     if rank == 0 and world == 1 and not args.no_extra:
+        line["four_cycle"] = four_cycle_leg(dg, dev, stream, flush, tune=not args.no_autotune)
         line["reference_gpu_kernel"] = ref_kernel_leg(host, dg, qs, want, dev)
         import bench_modes
         line["enumerate"] = bench_modes.enumerate_leg(warmup=1, steps=3)
@@ -587,6 +597,54 @@ def c1_leg(dev, cpu: bool) -> dict:
                                     "ms": res[hi["usable_cores"]] * 1e3, "ms_1_thread": res[1] * 1e3,
                                     "matches_per_s": c / res[hi["usable_cores"]]}
     return out
+
+
+def four_cycle_leg(dg, dev, stream, flush, tune: bool) -> dict:
+    """The single-query plain kernel on a 4-edge motif: the 4-cycle
+    0->1->2->3->0, delta 86400, count, on the bench graph (resident).  Device
+    time of the search kernel (CUDA events on the worker's stream), L2
+    flushed before every run, median of 5 after 2 warm-up runs, with the
+    autotuned launch parameters (tuned outside the timing) and with the
+    defaults; effective rate = the serial semantics' algorithmic bytes of
+    the query (12 roots + 8 r_reads + 16 candidates, counted by the oracle)
+    / kernel time, against the measured HBM copy bandwidth."""
+    import torch
+    from everest_b200 import autotune, capi, workloads
+    st = workload_stats("bursty-7.8m-4cycle")["queries"][0]
+    q = workloads.queries("bursty-7.8m-4cycle")[0]
+    peak, peak_kind = measured_peaks()
+    w = capi.Worker(dev, stream.cuda_stream)
+
+    def timed(flags):
+        ms = []
+        for i in range(7):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            w.take(dg, q["mu"], q["mv"], q["delta"], 0, -1, 0, flags)
+            c = w.run()
+            if c != st["count"]:
+                raise SystemExit(f"4-cycle count {c} != {st['count']}")
+            if i >= 2:
+                ms.append(w.last_stats()["device_ms"])
+        return statistics.median(ms)
+
+    try:
+        default_ms = timed(0)
+        cfg = dict(autotune.DEFAULT)
+        if tune:
+            cfg = autotune.Autotuner(dev, sample_roots=0).tune(dg, q["mu"], q["mv"], q["delta"], w)
+        flags = autotune.Autotuner.apply(w, cfg)
+        ms = timed(flags)
+    finally:
+        w.close()
+    ach = st["bytes_alg"] / (ms / 1e3) / 1e9
+    return {"workload": "bursty-1.1m-7.8m (the bench graph): 4-cycle 0->1->2->3->0, delta 86400, count",
+            "count": st["count"], "kernel_ms": ms, "kernel_ms_default_params": default_ms,
+            "tuning": "bps%d/steal%d/split%d/flags%d" % (cfg["blocks_per_sm"], cfg["steal_interval"],
+                                                       cfg["min_split"], cfg["flags"]),
+            "bytes_alg": st["bytes_alg"], "effective_gbs": ach, "peak_gbs": peak,
+            "frac": ach / peak, "peak_source": f"{peak_kind} hbm_gbs",
+            "l2": "flushed before every run (256 MB write)"}
 
 
 def run_single_query(args):

@@ -65,10 +65,16 @@ constexpr int kScanWide = EVX_SCAN_WIDE;
 #define EVX_PAIR_SIG 1
 #endif
 
+// Constrained launches pack the roots that pass their predicates into full
+// batches of 32 (0: a batch is the next 32 roots, passing or not).
+#ifndef EVX_ROOT_PACK
+#define EVX_ROOT_PACK 1
+#endif
+
 // resident blocks per SM the register budget aims for (deeper motifs keep
 // more per-level state live)
 #ifndef EVX_MINB3
-#define EVX_MINB3 8
+#define EVX_MINB3 10
 #endif
 #ifndef EVX_MINB4
 #define EVX_MINB4 7
@@ -1070,22 +1076,48 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
     const int rb = sm.q.root_beg + (t - sm.q.tile_beg) * la.tile_roots;
     const int re = min(rb + la.tile_roots, sm.q.root_end);
     const int delta = sm.q.delta;
-    for (int b0 = rb; b0 < re; b0 += 32) {
-      const int r = b0 + lane;
+    for (int b0 = rb; b0 < re;) {
       bool has = false;
-      if (r < re) {
-        const int4 ed = __ldg(g.edges + r);
-        bool ok = ed.x != ed.y;  // self-loops are not roots
-        if constexpr (CS) {
-          // the root is motif edge 0 = 0 -> 1: its edge and both node predicates
-          if (ok && la.cons.edge_ok) ok = __ldg(la.cons.edge_ok + r) != 0;
-          if (ok && la.cons.node_ok)
-            ok = ((__ldg(la.cons.node_ok + ed.x) & 1) != 0) && ((__ldg(la.cons.node_ok + ed.y) & 2) != 0);
+      if constexpr (CS) {
+        // the root is motif edge 0 = 0 -> 1: its edge and both node
+        // predicates.  Predicates reject most roots, so the roots that pass
+        // are packed into the batch until it holds 32 (or the tile ends),
+        // in edge order.
+        int n = 0;
+        while (n < 32 && b0 < re && (EVX_ROOT_PACK || n == 0)) {
+          const int r = b0 + lane;
+          bool ok = false;
+          int4 ed = make_int4(0, 0, 0, 0);
+          if (r < re) {
+            ed = __ldg(g.edges + r);
+            ok = ed.x != ed.y;  // self-loops are not roots
+            if (ok && la.cons.edge_ok) ok = __ldg(la.cons.edge_ok + r) != 0;
+            if (ok && la.cons.node_ok)
+              ok = ((__ldg(la.cons.node_ok + ed.x) & 1) != 0) && ((__ldg(la.cons.node_ok + ed.y) & 2) != 0);
+          }
+          const unsigned bm = __ballot_sync(kFull, ok);
+          const int rank = __popc(bm & S.lt), room = 32 - n;
+          int adv = min(32, re - b0), take = __popc(bm);
+          if (take > room) {
+            // the batch fills at the room-th passing root: resume after it
+            adv = __ffs(__ballot_sync(kFull, ok && rank == room - 1));
+            take = room;
+          }
+          if (ok && rank < room) sm.root[n + rank] = make_int4(ed.x, ed.y, ed.z + delta, r);
+          n += take;
+          b0 += adv;
         }
-        if (ok) {
-          sm.root[lane] = make_int4(ed.x, ed.y, ed.z + delta, r);
-          has = true;
+        has = lane < n;
+      } else {
+        const int r = b0 + lane;
+        if (r < re) {
+          const int4 ed = __ldg(g.edges + r);
+          if (ed.x != ed.y) {  // self-loops are not roots
+            sm.root[lane] = make_int4(ed.x, ed.y, ed.z + delta, r);
+            has = true;
+          }
         }
+        b0 += 32;
       }
       __syncwarp();
       if (!ENUM && S.kr() == 2 && (S.qf & kQInlineLast)) {

@@ -17,6 +17,8 @@ WORKLOADS: Dict[str, dict] = {
     # 1.1M nodes / 7.8M edges, every connected 3-edge pattern on 2-3 nodes
     # (36 by rule), each run separately, delta 86400, count
     "bursty-7.8m-3edge": {"graph": "bursty-1.1m-7.8m", "kind": "three_edge", "delta": 86400},
+    # the same graph, the 4-cycle 0->1->2->3->0, delta 86400, count
+    "bursty-7.8m-4cycle": {"graph": "bursty-1.1m-7.8m", "kind": "four_cycle", "delta": 86400},
 }
 
 
@@ -24,6 +26,8 @@ def queries(name: str) -> List[dict]:
     wl = WORKLOADS[name]
     if wl["kind"] == "triangle":
         return [{"name": "triangle", "mu": [0, 1, 2], "mv": [1, 2, 0], "delta": wl["delta"]}]
+    if wl["kind"] == "four_cycle":
+        return [{"name": "4-cycle", "mu": [0, 1, 2, 3], "mv": [1, 2, 3, 0], "delta": wl["delta"]}]
     if wl["kind"] == "three_edge":
         out = []
         for i, p in enumerate(synth.three_edge_patterns()):

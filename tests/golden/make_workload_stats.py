@@ -4,8 +4,9 @@ roots, CSR offset-pair reads, list openings and candidates examined, from
 which bytes_alg = 12 roots + 8 r_reads + 16 candidates.
 
 bench.py reads the JSON this writes (it never runs the oracle outside its
-cpu_baseline leg).  Run from the repository root:
-    python tests/golden/make_workload_stats.py
+cpu_baseline leg).  Run from the repository root (named workloads only, the
+others kept as they are in the JSON; all when none is named):
+    python tests/golden/make_workload_stats.py [workload ...]
 """
 import json
 import os
@@ -19,10 +20,14 @@ from oracle import oracle as O  # noqa: E402
 from everest_b200 import synth, workloads  # noqa: E402
 
 
-def main():
+def main(names):
+    path = os.path.join(HERE, "workload_stats.json")
     out = {}
+    if names and os.path.exists(path):
+        with open(path) as f:
+            out = json.load(f)
     for wname, wl in workloads.WORKLOADS.items():
-        if not wl.get("stats", True):
+        if not wl.get("stats", True) or (names and wname not in names):
             continue
         spec = synth.SPECS[wl["graph"]]
         u, v, t = synth.load_or_generate(spec.name)
@@ -35,9 +40,9 @@ def main():
                          "count": c, **st})
             print(wname, q["name"], c, flush=True)
         out[wname] = {"graph": spec.name, "queries": rows}
-    with open(os.path.join(HERE, "workload_stats.json"), "w") as f:
+    with open(path, "w") as f:
         json.dump(out, f, indent=1)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])
