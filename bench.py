@@ -98,7 +98,7 @@ def parse():
     ap.add_argument("--limit", type=float, default=None,
                     help="work limit per query, in adjacency records examined inside their time windows. "
                          "batch (default 0 = none, every result exact): stopped queries are flagged in both "
-                         "arms; serve (default 1e8): queries past it leave the shared batches for heavy slots")
+                         "arms; serve (default 3e7): queries past it leave the shared batches for heavy slots")
     return ap.parse_args()
 
 
@@ -466,7 +466,7 @@ def run_gpu_arm(args):
         # one-at-a-time arm (every query exact) and the Poisson pass stay
         # within a few minutes: a handful of 5-edge queries at deltas of days
         # take seconds alone even on such windows
-        line["serve"] = bench_modes.serve_leg(n=2000, window=1000, limit=int(1e8), warmup=0, steps=1)
+        line["serve"] = bench_modes.serve_leg(n=2000, window=1000, limit=int(3e7), warmup=0, steps=1)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         hi = host_info()
         threads = hi["usable_cores"]

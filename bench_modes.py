@@ -157,7 +157,7 @@ def run_batch(args) -> int:
     return 0
 
 
-def serve_leg(n: int = 10_000, window: int = 100_000, limit: int = int(1e8), warmup: int = 1, steps: int = 3,
+def serve_leg(n: int = 10_000, window: int = 100_000, limit: int = int(3e7), warmup: int = 1, steps: int = 3,
               slots: str = "64,2,2,2,1.0,2,2") -> dict:
     """Serving: a stream of n 3-5-edge count and enumerate queries on two
     resident graphs (7.8M and 63M edges; ``workloads.serve_queries``)
@@ -275,7 +275,7 @@ def serve_leg(n: int = 10_000, window: int = 100_000, limit: int = int(1e8), war
 def run_serve(args) -> int:
     """``bench.py --mode serve``: serve_leg as its own JSON line."""
     leg = serve_leg(n=args.queries or 10_000, window=args.window or 100_000,
-                    limit=int(args.limit if args.limit is not None else 1e8),
+                    limit=int(args.limit if args.limit is not None else 3e7),
                     warmup=args.warmup, steps=args.steps, slots=getattr(args, "serve_slots", "64,2,2,2,1.0,2,2"))
     line = {"metric": leg["metric"], "value": leg["value"], "unit": "queries/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup,

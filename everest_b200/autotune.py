@@ -13,8 +13,9 @@ Knobs: resident blocks per SM (0 = occupancy), intra-warp rebalance interval
 and minimum split width ("steal granularity"), how the last edge is
 counted: range arithmetic on the pair index, a pair hash-table or
 pair-directory lookup per partial match, or a scan ("tail-expansion depth"),
-and whether an edge between two mapped nodes walks its pair run or scans the
-shorter adjacency list.  Batches are tuned on
+whether an edge between two mapped nodes walks its pair run or scans the
+shorter adjacency list, and whether each root's window is bounded by the
+last edge's list.  Batches are tuned on
 their tile size.
 """
 from __future__ import annotations
@@ -42,6 +43,8 @@ CANDIDATES = [
     {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_NEW_SCAN},
     {"blocks_per_sm": 4, "steal_interval": 16, "min_split": 2, "flags": 0},
     {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_LIST_SCAN},
+    {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_NO_ROOT_BOUND},
+    {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_NO_ROOT_BOUND},
 ]
 BATCH_TILES = (64, 128, 256, 512)
 

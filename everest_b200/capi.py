@@ -34,6 +34,7 @@ FLAG_NEW_SCAN = 128
 FLAG_LIST_SCAN = 256
 FLAG_PER_LANE = 512
 FLAG_WARP_SYNC = 1024
+FLAG_NO_ROOT_BOUND = 2048
 MAX_MOTIF_EDGES = 8
 
 # every symbol include/everest_b200.h declares

@@ -104,11 +104,13 @@ int build_plan(int k, const int *mu, const int *mv, MotifPlan *plan) {
 // closing edge whose pair changes with every partial match: one lookup per
 // partial match in the pair hash table (kQPairHash, the default) or, on
 // request, in the per-node pair directory (kQPairDir).  kQNoPrune turns off
-// the check of the closing edge's fixed endpoint before a task's scan.  A last
+// the check of the closing edge's fixed endpoint before a task's scan, and
+// kQNoBound the per-root window bound from the last edge's list.  A last
 // edge that maps a new node is scanned, and past the first step of a window
 // the rest is counted by range arithmetic (kQNewArith) unless asked not to.
 int tail_mode(const MotifPlan &plan, unsigned flags, bool enumerate) {
   const int np = ((flags & EVX_FLAG_NO_CLOSING_PRUNE) ? kQNoPrune : 0) |
+                 ((flags & EVX_FLAG_NO_ROOT_BOUND) ? kQNoBound : 0) |
                  ((flags & (EVX_FLAG_LIST_SCAN | EVX_FLAG_NO_PAIR_INDEX | EVX_FLAG_CLOSING_SCAN)) ? 0 : kQPairScan);
   const int k = plan.k;
   if (enumerate || (flags & EVX_FLAG_NO_PAIR_INDEX) || k < 2) return np;

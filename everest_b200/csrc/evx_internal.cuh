@@ -122,6 +122,7 @@ constexpr int kQNoPrune = 32;    // no closing-endpoint check before a task's sc
 constexpr int kQRevPair = 64;    // last edge reverses the previous edge's endpoints
 constexpr int kQNewArith = 128;  // a new-node last edge's long windows counted by range arithmetic
 constexpr int kQPairScan = 256;  // a scanned edge between two mapped nodes walks its pair run
+constexpr int kQNoBound = 512;   // no per-root window bound from the last edge's list
 struct QueryDesc {
   MotifPlan plan;
   int root_beg, root_end;  // root edge ids [beg, end)

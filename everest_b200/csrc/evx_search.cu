@@ -65,8 +65,31 @@ constexpr int kScanWide = EVX_SCAN_WIDE;
 #define EVX_PAIR_SIG 1
 #endif
 
-// Constrained launches pack the roots that pass their predicates into full
-// batches of 32 (0: a batch is the next 32 roots, passing or not).
+// A list search for the first record after the previous edge starts from
+// the root edge's own position when the list belongs to one of the root
+// edge's endpoints (known without a search), galloping up from there; 0:
+// a binary search over the whole list.
+#ifndef EVX_ROOT_GALLOP
+#define EVX_ROOT_GALLOP 1
+#endif
+
+// Window end per root from the last motif edge: when that edge has a root
+// node as its source (target), it lies in the root node's out-list (in-list)
+// after the root edge and inside the window, so every edge of a match is at
+// most the last such entry.  When the window holds at most EVX_BOUND_MAX
+// of them, that entry's timestamp becomes the root's window end (the same
+// matches: the window only loses edges no match can use), and a root with
+// none is dropped before it takes a lane.  0: off.
+#ifndef EVX_ROOT_BOUND
+#define EVX_ROOT_BOUND 1
+#endif
+#ifndef EVX_BOUND_MAX
+#define EVX_BOUND_MAX 32
+#endif
+
+// Roots that pass (not a self-loop, the predicates of a constrained launch,
+// the window bound) are packed into full batches of 32 (0: a batch is the
+// next 32 roots, passing or not).
 #ifndef EVX_ROOT_PACK
 #define EVX_ROOT_PACK 1
 #endif
@@ -220,6 +243,23 @@ __device__ __forceinline__ int list_first_t_after(const int4 *lst, int lo, int h
   return lo;
 }
 
+// First position in [lo, hi) of an adjacency list whose edge id is greater
+// than key, galloping up from lo.
+__device__ __forceinline__ int list_first_eid_after(const int4 *lst, int lo, int hi, int key) {
+  int step = 1;
+  while (lo < hi) {
+    const int probe = min(lo + step - 1, hi - 1);
+    if (ld_eid(lst + probe) > key) { hi = probe; break; }
+    lo = probe + 1;
+    step <<= 1;
+  }
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ld_eid(lst + mid) > key) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
 // Entries of the pair run [start, start + len) whose edge id lies in [klo, khi].
 __device__ __forceinline__ int pair_count_eids(const GraphView &g, int start, int len, int klo, int khi) {
   if (len <= 0) return 0;
@@ -366,6 +406,16 @@ struct Searcher {
     return p.dst == x ? p.pip + 1 : (p.src == x ? __ldg(g.cross_in + p.eid) : -1);
   }
 
+  // First position of out(x) / in(x) after the root edge (x one of its
+  // endpoints), else -1: every later edge of the partial match comes after
+  // it, so a search for the first record after the previous edge can start
+  // there.
+  __device__ __forceinline__ int after_root(int root, int x, bool outl) const {
+    const int4 rt = sm.root[root];
+    if (outl) return x == rt.x ? __ldg(&g.edges[rt.w].w) + 1 : (x == rt.y ? __ldg(g.cross_out + rt.w) : -1);
+    return x == rt.y ? __ldg(g.inpos + rt.w) + 1 : (x == rt.x ? __ldg(g.cross_in + rt.w) : -1);
+  }
+
   // Constrained queries (CS): a candidate also needs its edge predicate and,
   // when it maps a new motif node (want < 0), that node's predicate (bit nmc
   // of its mask: the new node's index is the number mapped before it).
@@ -504,7 +554,7 @@ struct Searcher {
     int stride = 1;  // distance between this lane's records (interleaved slices)
     bool out = true;
     bool prun = false;  // the range is a run of pair_rec (the edge's static pair), not a list
-    int blo = 0, bhi = 0;
+    int blo = 0, bhi = 0, gstep = 0;
     bool searching = false;
     if (PS && has && kind == 2 && (qf & kQPairScan)) {
       // both endpoints are mapped: walk the run of the static edge (ia, ib)
@@ -555,19 +605,26 @@ struct Searcher {
         pos = sc;
       } else if (lo < hi) {
         blo = lo; bhi = hi; searching = true;
+        if (EVX_ROOT_GALLOP && l > 0 && !strict_()) {
+          const int fr = after_root(root, base, out);
+          if (fr >= 0) { blo = fr; gstep = 1; }
+          if (blo >= bhi) { searching = false; pos = bhi; }
+        }
       } else {
         pos = hi;
       }
     }
-    // first record after the previous edge (by id; by time in strict mode)
+    // first record after the previous edge (by id; by time in strict mode):
+    // galloping up from the root edge's position while gstep > 0, then
+    // halving
     {
       const int key = strict_() ? p.t : p.eid;
       while (__any_sync(kFull, searching)) {
         if (searching) {
           const int4 *lst = out ? g.out_rec : g.in_rec;
-          const int mid = (blo + bhi) >> 1;
+          const int mid = gstep > 0 ? min(blo + gstep - 1, bhi - 1) : (blo + bhi) >> 1;
           const int v = strict_() ? ld_t(lst + mid) : ld_eid(lst + mid);
-          if (v > key) bhi = mid; else blo = mid + 1;
+          if (v > key) { bhi = mid; gstep = 0; } else { blo = mid + 1; gstep <<= 1; }
           if (blo >= bhi) { searching = false; pos = blo; }
         }
       }
@@ -715,7 +772,9 @@ struct Searcher {
         const int4 *lst = fa ? g.out_rec : g.in_rec;
         const int key = strict_() ? p.t : p.eid;
         const int known = strict_() ? -1 : (fa ? out_start(p, x) : in_start(p, x));
+        const int fr = (EVX_ROOT_GALLOP && known < 0 && !strict_() && l > 0) ? after_root(root, x, fa) : -1;
         if (known >= 0) lo = known;
+        else if (fr >= 0) lo = list_first_eid_after(lst, fr, hi, key);
         else {
           while (lo < hi) {
             const int mid = (lo + hi) >> 1;
@@ -1076,49 +1135,65 @@ search_kernel(const GraphView g, const __grid_constant__ QueryDesc q0, const Lau
     const int rb = sm.q.root_beg + (t - sm.q.tile_beg) * la.tile_roots;
     const int re = min(rb + la.tile_roots, sm.q.root_end);
     const int delta = sm.q.delta;
+    // the list that bounds each root's window (the last motif edge's list
+    // at a root node): 0 / 1 in-list of root node 0 / 1, 2 / 3 out-list of
+    // root node 0 / 1, -1 none
+    int side = -1;
+    if (EVX_ROOT_BOUND && S.kr() >= 3 && !(S.qf & kQNoBound)) {
+      const int wl = sm.q.plan.info[S.kr() - 2];
+      const int a = plan_a(wl), b = plan_b(wl);
+      side = b <= 1 ? b : (a <= 1 ? 2 + a : -1);
+    }
     for (int b0 = rb; b0 < re;) {
-      bool has = false;
-      if constexpr (CS) {
-        // the root is motif edge 0 = 0 -> 1: its edge and both node
-        // predicates.  Predicates reject most roots, so the roots that pass
-        // are packed into the batch until it holds 32 (or the tile ends),
-        // in edge order.
-        int n = 0;
-        while (n < 32 && b0 < re && (EVX_ROOT_PACK || n == 0)) {
-          const int r = b0 + lane;
-          bool ok = false;
-          int4 ed = make_int4(0, 0, 0, 0);
-          if (r < re) {
-            ed = __ldg(g.edges + r);
-            ok = ed.x != ed.y;  // self-loops are not roots
+      // The roots of the next batch, packed in edge order until it holds
+      // 32 or the tile ends: a root is an edge that is not a self-loop
+      // (with constraints: that passes its edge predicate and node
+      // predicates 0 and 1) and whose bounding list holds an entry inside
+      // its window.
+      int n = 0;
+      while (n < 32 && b0 < re && (EVX_ROOT_PACK || n == 0)) {
+        const int r = b0 + lane;
+        bool ok = false;
+        int4 ed = make_int4(0, 0, 0, 0);
+        int tlr = 0;
+        if (r < re) {
+          ed = __ldg(g.edges + r);
+          ok = ed.x != ed.y;
+          if constexpr (CS) {
             if (ok && la.cons.edge_ok) ok = __ldg(la.cons.edge_ok + r) != 0;
             if (ok && la.cons.node_ok)
               ok = ((__ldg(la.cons.node_ok + ed.x) & 1) != 0) && ((__ldg(la.cons.node_ok + ed.y) & 2) != 0);
           }
-          const unsigned bm = __ballot_sync(kFull, ok);
-          const int rank = __popc(bm & S.lt), room = 32 - n;
-          int adv = min(32, re - b0), take = __popc(bm);
-          if (take > room) {
-            // the batch fills at the room-th passing root: resume after it
-            adv = __ffs(__ballot_sync(kFull, ok && rank == room - 1));
-            take = room;
-          }
-          if (ok && rank < room) sm.root[n + rank] = make_int4(ed.x, ed.y, ed.z + delta, r);
-          n += take;
-          b0 += adv;
-        }
-        has = lane < n;
-      } else {
-        const int r = b0 + lane;
-        if (r < re) {
-          const int4 ed = __ldg(g.edges + r);
-          if (ed.x != ed.y) {  // self-loops are not roots
-            sm.root[lane] = make_int4(ed.x, ed.y, ed.z + delta, r);
-            has = true;
+          tlr = ed.z + delta;
+          if (ok && side >= 0) {
+            const int4 rg = __ldg(g.node_rng + ((side & 1) ? ed.y : ed.x));
+            int st, hi;
+            const int4 *lst;
+            if (side < 2) {
+              lst = g.in_rec; hi = rg.w;
+              st = side == 0 ? __ldg(g.cross_in + r) : __ldg(g.inpos + r) + 1;
+            } else {
+              lst = g.out_rec; hi = rg.y;
+              st = side == 2 ? ed.w + 1 : __ldg(g.cross_out + r);
+            }
+            const int nb = list_first_t_after(lst, st, min(hi, st + EVX_BOUND_MAX + 1), tlr) - st;
+            if (nb == 0) ok = false;
+            else if (nb <= EVX_BOUND_MAX) tlr = ld_t(lst + st + nb - 1);
           }
         }
-        b0 += 32;
+        const unsigned bm = __ballot_sync(kFull, ok);
+        const int rank = __popc(bm & S.lt), room = 32 - n;
+        int adv = min(32, re - b0), take = __popc(bm);
+        if (take > room) {
+          // the batch fills at the room-th passing root: resume after it
+          adv = __ffs(__ballot_sync(kFull, ok && rank == room - 1));
+          take = room;
+        }
+        if (ok && rank < room) sm.root[n + rank] = make_int4(ed.x, ed.y, tlr, r);
+        n += take;
+        b0 += adv;
       }
+      const bool has = lane < n;
       __syncwarp();
       if (!ENUM && S.kr() == 2 && (S.qf & kQInlineLast)) {
         // the only searched edge closes on the root's endpoints

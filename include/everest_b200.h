@@ -65,6 +65,10 @@ extern "C" {
  * This scans the shorter of out(u) / in(v) instead, as the reference does
  * (system/templates/common/resolveMi.snp:9-28). */
 #define EVX_FLAG_LIST_SCAN 256u
+/* When the last motif edge has a root node as an endpoint, each root's
+ * window ends at that node's last entry inside it (a root with none is
+ * skipped); this keeps the plain window (same results, for timing). */
+#define EVX_FLAG_NO_ROOT_BOUND 2048u
 /* evx_worker_take_constrained: a query with node predicates alone runs on
  * the warp-synchronous search, one with an edge predicate or temporal gaps
  * (and no anti-edge or filter) on the per-lane search.  EVX_FLAG_PER_LANE

@@ -74,6 +74,10 @@ def test_golden_small_graph_counts(golden, small_graphs, worker):
                 got6 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
                                  flags=capi.FLAG_LIST_SCAN)
                 assert got6 == c["count"], (gname, c["motif"], c["delta"], got6, "list scan")
+            if n % 8 == 3:  # without the per-root window bound on a subset
+                got7 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
+                                 flags=capi.FLAG_NO_ROOT_BOUND)
+                assert got7 == c["count"], (gname, c["motif"], c["delta"], got7, "no root bound")
             if n % 7 == 0:  # the scanning last level on a subset
                 got2 = gpu_count(worker, dg, c["mu"], c["mv"], c["delta"], rb, re_,
                                  flags=capi.FLAG_NO_PAIR_INDEX)
@@ -136,12 +140,14 @@ def test_random_tiny_vs_brute_force(worker):
         dg = device_graph(u, v, t)
         for flags in (0, capi.FLAG_NO_STEAL, capi.FLAG_NO_PAIR_INDEX, capi.FLAG_PAIR_DIR, capi.FLAG_CLOSING_SCAN,
                       capi.FLAG_NO_CLOSING_PRUNE, capi.FLAG_NO_CLOSING_PRUNE | capi.FLAG_NO_PAIR_INDEX,
-                      capi.FLAG_LIST_SCAN, capi.FLAG_LIST_SCAN | capi.FLAG_NO_STEAL):
+                      capi.FLAG_LIST_SCAN, capi.FLAG_LIST_SCAN | capi.FLAG_NO_STEAL, capi.FLAG_NO_ROOT_BOUND,
+                      capi.FLAG_NO_ROOT_BOUND | capi.FLAG_NO_PAIR_INDEX):
             assert gpu_count(worker, dg, mu, mv, delta, flags=flags) == want, (trial, pat, delta, flags)
         strict = len(O.brute_force(u, v, t, mu, mv, delta, strict_ts=True))
         assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS) == strict
         assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS | capi.FLAG_CLOSING_SCAN) == strict
         assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS | capi.FLAG_LIST_SCAN) == strict
+        assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS | capi.FLAG_NO_ROOT_BOUND) == strict
         dg.free()
 
 
@@ -276,7 +282,7 @@ def test_enumeration_random_tiny_vs_brute_force(worker):
         delta = int(rng.integers(0, 9))
         want = sorted(map(tuple, O.brute_force(u, v, t, mu, mv, delta)))
         dg = device_graph(u, v, t)
-        for flags in (0, capi.FLAG_LIST_SCAN, capi.FLAG_NO_STEAL):
+        for flags in (0, capi.FLAG_LIST_SCAN, capi.FLAG_NO_STEAL, capi.FLAG_NO_ROOT_BOUND):
             worker.take(dg, mu, mv, delta, 0, -1, len(want) + 4, flags)
             assert worker.run() == len(want), (trial, mu, mv, delta, flags)
             got = sorted(map(tuple, worker.enum_rows(len(want) + 4).tolist()))
