@@ -75,7 +75,9 @@ class _KernelGen:
         shutil.copytree(os.path.join(ref_root, "system"), os.path.join(self.scratch, "system"))
         pkg = types.ModuleType("tmine")
         pkg.__path__ = [os.path.join(self.scratch, "system", "tmine")]
-        self._saved = sys.modules.get("tmine")
+        self._saved = {m: mod for m, mod in sys.modules.items() if m == "tmine" or m.startswith("tmine.")}
+        for m in self._saved:
+            del sys.modules[m]
         sys.modules["tmine"] = pkg
         from tmine import KernelGen as KG, Query as Q  # noqa: E402
         self.KG, self.Q = KG, Q
@@ -100,10 +102,9 @@ class _KernelGen:
 
     def close(self) -> None:
         shutil.rmtree(self.scratch, ignore_errors=True)
-        if self._saved is None:
-            sys.modules.pop("tmine", None)
-        else:
-            sys.modules["tmine"] = self._saved
+        for m in [m for m in sys.modules if m == "tmine" or m.startswith("tmine.")]:
+            del sys.modules[m]
+        sys.modules.update(self._saved)
 
 
 def patch(src: str) -> str:

@@ -44,6 +44,12 @@ def available() -> bool:
     return reference_root() is not None
 
 
+def _drop_tmine() -> None:
+    """Forget the tmine package and its submodules imported from a scratch copy."""
+    for name in [m for m in sys.modules if m == "tmine" or m.startswith("tmine.")]:
+        del sys.modules[name]
+
+
 def _kernelgen():
     """KernelGen and Query from a scratch copy of the reference's system/."""
     global _kg
@@ -55,6 +61,7 @@ def _kernelgen():
         shutil.copytree(os.path.join(ref, "system"), os.path.join(scratch, "system"))
         pkg = types.ModuleType("tmine")
         pkg.__path__ = [os.path.join(scratch, "system", "tmine")]
+        _drop_tmine()  # submodules another scratch copy left behind
         sys.modules["tmine"] = pkg  # bypass tmine/__init__ (it imports the compiled corelib)
         from tmine import KernelGen as KG, Query as Q  # noqa: E402
         _kg = (KG, Q, scratch)
@@ -66,7 +73,7 @@ def cleanup() -> None:
     global _kg
     if _kg is not None:
         shutil.rmtree(_kg[2], ignore_errors=True)
-        sys.modules.pop("tmine", None)
+        _drop_tmine()
         _kg = None
 
 
