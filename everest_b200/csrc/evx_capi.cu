@@ -599,14 +599,15 @@ int evx_worker_take_constrained(evx_worker *w, const evx_graph *gh, int k, const
   rc = cons_build_masks(*c, plan.n, g.node_feat, (int)V, g.edge_feat, (int)E, w->node_ok_d, w->edge_ok_d,
                         w->num_sms, w->stream);
   if (rc) return rc;
-  // Node predicates alone run on the warp-synchronous search with the checks
-  // compiled in (the CS kernels), where range arithmetic still counts
-  // closing last edges; with an edge predicate or temporal gaps it counts
-  // nothing by ranges and the per-lane search measured faster (the 4-cycle
-  // with gaps on 7.8M edges: 2.3 vs 3.7 ms), so those take the per-lane
-  // search unless EVX_FLAG_WARP_SYNC asks otherwise.
+  // Node and edge predicates and temporal gaps run on the warp-synchronous
+  // search with the checks compiled in (the CS kernels), where range
+  // arithmetic still counts closing last edges under node predicates alone
+  // (on 7.8M edges, the 4-cycle with node predicates and gaps: 1.25 ms
+  // against 2.17 ms per lane; with an edge predicate: 3.8 against 6.5 ms);
+  // anti-edges and filters take the per-lane search, and EVX_FLAG_PER_LANE
+  // sends any query there.
   const bool ws_ok = c->anti_mask == 0 && !c->has_filter && !(flags & EVX_FLAG_PER_LANE);
-  if (ws_ok && ((!c->has_edge && !c->has_temporal) || (flags & EVX_FLAG_WARP_SYNC))) {
+  if (ws_ok) {
     // Range arithmetic counts edges without looking at them, so it stays
     // only where no counted edge has a check: closing last edges under node
     // predicates alone.

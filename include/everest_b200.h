@@ -69,11 +69,10 @@ extern "C" {
  * window ends at that node's last entry inside it (a root with none is
  * skipped); this keeps the plain window (same results, for timing). */
 #define EVX_FLAG_NO_ROOT_BOUND 2048u
-/* evx_worker_take_constrained: a query with node predicates alone runs on
- * the warp-synchronous search, one with an edge predicate or temporal gaps
- * (and no anti-edge or filter) on the per-lane search.  EVX_FLAG_PER_LANE
- * sends the first kind to the per-lane search too; EVX_FLAG_WARP_SYNC sends
- * the second kind to the warp-synchronous search. */
+/* evx_worker_take_constrained: a query without anti-edges or a filter (node
+ * and edge predicates, temporal gaps) runs on the warp-synchronous search;
+ * EVX_FLAG_PER_LANE sends it to the per-lane search instead.
+ * EVX_FLAG_WARP_SYNC asks for the warp-synchronous search, the default. */
 #define EVX_FLAG_PER_LANE 512u
 #define EVX_FLAG_WARP_SYNC 1024u
 
@@ -361,10 +360,10 @@ EVX_API int evx_graph_set_features(evx_graph *g, const int *node_features, const
  * an anti-edge, and enumeration with anti-edges (its rows would name no
  * edge); node / edge predicates need the matching features on the graph.
  * Flags: EVX_FLAG_EXACT_TOTAL, EVX_FLAG_PER_LANE and EVX_FLAG_WARP_SYNC
- * only.  A query with node predicates alone runs on the warp-synchronous
- * search with the checks compiled in; anti-edges or a filter take the
- * per-lane constrained search, and so do edge predicates and temporal gaps
- * unless EVX_FLAG_WARP_SYNC is given.  The plain search's launch, result and rows
+ * only.  A query without anti-edges or a filter runs on the
+ * warp-synchronous search with the checks compiled in (the per-lane
+ * constrained search with EVX_FLAG_PER_LANE); anti-edges or a filter take
+ * the per-lane constrained search.  The plain search's launch, result and rows
  * calls then run this job; the work limit (evx_worker_set_limit) does not
  * apply to it.  A struct with no constraint set runs the plain search. */
 EVX_API int evx_worker_take_constrained(evx_worker *w, const evx_graph *g, int k, const int *mu,
