@@ -176,6 +176,11 @@ __device__ __forceinline__ int first_eid_after(const int4 *__restrict__ recs, in
 // its own column, so the dynamically indexed levels cost shared-memory
 // accesses (conflict-free: 32 lanes, 32 consecutive words) instead of a
 // local-memory stack.
+// Roots whose last motif edge cannot occur are dropped at the claim (0: off).
+#ifndef EVX_CONS_ROOT_DROP
+#define EVX_CONS_ROOT_DROP 1
+#endif
+
 template <int K>
 struct ConsWarpState {
   int m[K + 1][32];             // graph node of each motif node
@@ -195,6 +200,20 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
   auto pos = [&](int i) -> int & { return W.pos[i][lane]; };
   auto endp = [&](int i) -> int & { return W.endp[i][lane]; };
   auto tlv = [&](int i) -> int & { return W.tlv[i][lane]; };
+  // The last motif edge is real (never an anti-edge).  When it has a root
+  // node as its source (target), it lies in that node's out-list (in-list)
+  // after the root edge and inside its window, which ends t(e_0) + delta
+  // after the root (t(e_0) + gap_0 for a two-edge motif with gaps: edge 1's
+  // window may pass delta): a root whose list holds no such entry has no
+  // match and is not searched.  side: 0 / 1 in-list of root node 0 / 1,
+  // 2 / 3 out-list of root node 0 / 1, -1 none.
+  const int last_win = (K == 2 && s.has_temporal) ? s.temporal[0] : s.delta;
+  int side = -1;
+  if (EVX_CONS_ROOT_DROP) {
+    const int wl = s.plan.info[K - 2];
+    const int la = plan_a(wl), lb = plan_b(wl);
+    side = lb <= 1 ? lb : (la <= 1 ? 2 + la : -1);
+  }
   unsigned useout = 0;      // bit j: motif edge j scans an out-list
   int j = 0;                // motif edge being scanned; 0 = between roots
   bool done = false;        // no roots left for this lane
@@ -260,6 +279,19 @@ __global__ void __launch_bounds__(kConsBlock) cons_search_kernel(const GraphView
             ok = ((__ldg(s.node_ok + e.x) & 1) != 0) && ((__ldg(s.node_ok + e.y) & 2) != 0);
           }
           if (ok && s.edge_ok) ok = __ldg(s.edge_ok + r) != 0;
+          if (ok && side >= 0) {
+            const int4 rg = __ldg(g.node_rng + ((side & 1) ? e.y : e.x));
+            int st, hi2;
+            const int4 *lst;
+            if (side < 2) {
+              lst = g.in_rec; hi2 = rg.w;
+              st = side == 0 ? __ldg(g.cross_in + r) : __ldg(g.inpos + r) + 1;
+            } else {
+              lst = g.out_rec; hi2 = rg.y;
+              st = side == 2 ? e.w + 1 : __ldg(g.cross_out + r);
+            }
+            ok = st < hi2 && __ldg(&lst[st].z) <= e.z + last_win;
+          }
           if (ok) {
             m(0) = e.x;
             m(1) = e.y;
