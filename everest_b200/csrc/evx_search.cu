@@ -87,6 +87,12 @@ constexpr int kScanWide = EVX_SCAN_WIDE;
 #define EVX_BOUND_MAX 32
 #endif
 
+// Same-pair / reverse-pair tails inline at a level queue their lookups and
+// count them 32 at a time (0: each lane looks its candidates up itself).
+#ifndef EVX_TAIL_QUEUE
+#define EVX_TAIL_QUEUE 1
+#endif
+
 // Roots that pass (not a self-loop, the predicates of a constrained launch,
 // the window bound) are packed into full batches of 32 (0: a batch is the
 // next 32 roots, passing or not).
@@ -915,19 +921,37 @@ struct Searcher {
             // a candidate whose record says its own pair's run (top bit) or
             // its reverse pair's run (kRevLater) has no entry after it adds
             // nothing: skip its lookup
-            int2 pl[kScanWide];
             const int later = rev ? kRevLater : (int)0x80000000u;
+            if (EVX_TAIL_QUEUE && !strict_()) {
+              // queue them (edge id, window end) in the next level's unused
+              // task buffer and count them 32 at a time
 #pragma unroll
-            for (int q = 0; q < kScanWide; q++) {
-              if (!prun && !(rw[q].w & later)) ok[q] = false;
-              pl[q] = ok[q] ? __ldg((rev ? g.rev_loc : g.pair_loc) + rw[q].x) : make_int2(0, 0);
-            }
+              for (int q = 0; q < kScanWide; q++) {
+                const bool push = ok[q] && (prun || (rw[q].w & later));
+                const unsigned pm = __ballot_sync(kFull, push);
+                if (pm) {
+                  const int nb = sm.nb[l + 1];
+                  if (push) sm.task[l][nb + __popc(pm & lt)][0] = make_int4(rw[q].x, tl, 0, 0);
+                  __syncwarp();
+                  if (lane == 0) sm.nb[l + 1] = nb + __popc(pm);
+                  __syncwarp();
+                  if (nb + __popc(pm) >= 32) tail_batch<l>(rev, false);
+                }
+              }
+            } else {
+              int2 pl[kScanWide];
 #pragma unroll
-            for (int q = 0; q < kScanWide; q++) {
-              if (ok[q]) {
-                int lo = rev ? pl[q].x : pl[q].x + 1;
-                if (strict_()) lo = pair_first_t_after(g, lo, pl[q].y, rw[q].z);
-                cnt += (unsigned long long)(pair_gallop_t_after(g, lo, pl[q].y, tl) - lo);
+              for (int q = 0; q < kScanWide; q++) {
+                if (!prun && !(rw[q].w & later)) ok[q] = false;
+                pl[q] = ok[q] ? __ldg((rev ? g.rev_loc : g.pair_loc) + rw[q].x) : make_int2(0, 0);
+              }
+#pragma unroll
+              for (int q = 0; q < kScanWide; q++) {
+                if (ok[q]) {
+                  int lo = rev ? pl[q].x : pl[q].x + 1;
+                  if (strict_()) lo = pair_first_t_after(g, lo, pl[q].y, rw[q].z);
+                  cnt += (unsigned long long)(pair_gallop_t_after(g, lo, pl[q].y, tl) - lo);
+                }
               }
             }
           } else {
@@ -974,6 +998,48 @@ struct Searcher {
             if (sm.nb[l + 1] >= 32) break;  // descend before the next push
           }
         }
+      }
+      if (EVX_TAIL_QUEUE && inline_here && (qf & (kQSamePair | kQRevPair)) && !strict_()) {
+        // the queued tail lookups left over (none when the query stopped)
+        if (sm.halt) {
+          __syncwarp();
+          if (lane == 0) sm.nb[l + 1] = 0;
+          __syncwarp();
+        } else {
+          tail_batch<l>((qf & kQRevPair) != 0, true);
+        }
+      }
+    }
+  }
+
+  // Count the queued same-pair / reverse-pair tail lookups of level l (in
+  // the task buffer of level l + 1, which an inline level leaves unused):
+  // 32 at a time, each lane one entry {edge id, window end}: the entries of
+  // the edge's own pair run (reverse pair's run) after it and inside the
+  // window.  all: until the queue is empty, else one batch.  At most 63
+  // entries are queued when it is called.
+  template <int l>
+  __device__ __forceinline__ void tail_batch(bool rev, bool all) {
+    if constexpr (l < L - 1) {
+      while (true) {
+        const int nb = sm.nb[l + 1];
+        if (nb == 0) break;
+        const int take = nb < 32 ? nb : 32;
+        if (lane < take) {
+          const int4 qe = sm.task[l][lane][0];
+          const int2 pl = __ldg((rev ? g.rev_loc : g.pair_loc) + qe.x);
+          const int lo = rev ? pl.x : pl.x + 1;
+          cnt += (unsigned long long)(pair_gallop_t_after(g, lo, pl.y, qe.y) - lo);
+        }
+        __syncwarp();
+        const int rest = nb - take;
+        int4 a = make_int4(0, 0, 0, 0);
+        if (lane < rest) a = sm.task[l][take + lane][0];
+        __syncwarp();
+        if (lane < rest) sm.task[l][lane][0] = a;
+        if (lane == 0) sm.nb[l + 1] = rest;
+        __syncwarp();
+        if (!all) break;
       }
     }
   }
