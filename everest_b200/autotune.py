@@ -45,6 +45,11 @@ CANDIDATES = [
     {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_LIST_SCAN},
     {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_NO_ROOT_BOUND},
     {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_NO_ROOT_BOUND},
+    {"blocks_per_sm": 0, "steal_interval": 64, "min_split": 4, "flags": capi.FLAG_NO_ROOT_BOUND},
+    {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2,
+     "flags": capi.FLAG_NO_CLOSING_PRUNE | capi.FLAG_NO_ROOT_BOUND},
+    {"blocks_per_sm": 0, "steal_interval": 4, "min_split": 2, "flags": capi.FLAG_NEW_SCAN | capi.FLAG_NO_ROOT_BOUND},
+    {"blocks_per_sm": 0, "steal_interval": 16, "min_split": 2, "flags": capi.FLAG_PAIR_DIR | capi.FLAG_NO_ROOT_BOUND},
 ]
 BATCH_TILES = (64, 128, 256, 512)
 

@@ -141,7 +141,9 @@ def test_random_tiny_vs_brute_force(worker):
         for flags in (0, capi.FLAG_NO_STEAL, capi.FLAG_NO_PAIR_INDEX, capi.FLAG_PAIR_DIR, capi.FLAG_CLOSING_SCAN,
                       capi.FLAG_NO_CLOSING_PRUNE, capi.FLAG_NO_CLOSING_PRUNE | capi.FLAG_NO_PAIR_INDEX,
                       capi.FLAG_LIST_SCAN, capi.FLAG_LIST_SCAN | capi.FLAG_NO_STEAL, capi.FLAG_NO_ROOT_BOUND,
-                      capi.FLAG_NO_ROOT_BOUND | capi.FLAG_NO_PAIR_INDEX):
+                      capi.FLAG_NO_ROOT_BOUND | capi.FLAG_NO_PAIR_INDEX,
+                      capi.FLAG_NO_ROOT_BOUND | capi.FLAG_NO_CLOSING_PRUNE, capi.FLAG_NO_ROOT_BOUND | capi.FLAG_NEW_SCAN,
+                      capi.FLAG_NO_ROOT_BOUND | capi.FLAG_PAIR_DIR):
             assert gpu_count(worker, dg, mu, mv, delta, flags=flags) == want, (trial, pat, delta, flags)
         strict = len(O.brute_force(u, v, t, mu, mv, delta, strict_ts=True))
         assert gpu_count(worker, dg, mu, mv, delta, flags=capi.FLAG_STRICT_TS) == strict
