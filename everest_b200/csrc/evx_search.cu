@@ -34,6 +34,11 @@
 //    one-candidate-per-thief split (system/templates/warpBalancing/top.snp)
 //    and its host-driven dump/expand rounds (system/templates/tailExpan/Expanding.snp);
 //  * the last level reads several records per lane per step (count mode);
+//  * a root whose last motif edge has no candidate in its root node's list
+//    inside the window is dropped before it takes a lane, the others' windows
+//    end at that list's last entry, and the roots that remain are packed into
+//    full batches of 32;
+//  * same-pair / reverse-pair tails are queued and counted 32 at a time;
 //  * enumeration slots are reserved with one warp-aggregated atomicAdd per
 //    step (the reference issues one atomicAdd per match,
 //    system/tmine/KernelGen.py:505-524).
